@@ -1,0 +1,257 @@
+/*
+ * graphite_b200.h -- C ABI of libgraphite_b200.so, a B200 (sm_100a)
+ * implementation of the explicit second-order unstructured finite-volume
+ * Euler iteration of Alexsimulation/graphite.
+ *
+ * The entry points keep the names, argument meaning and call order of the
+ * reference's mesh, field and FvmEuler* functions (the surface apps/main.cu
+ * drives through PhysicsEuler), with C linkage so that any FFI can bind them:
+ *
+ *   cuMeshFromSu2 -> cuMeshFromFile -> FvmFieldNew x4 -> FvmEulerInit
+ *   per iteration: FvmEulerSlipBc / FvmEulerInletOutletBc per region
+ *                  -> FvmEulerStepPrepare -> FvmEulerStep -> FvmFieldReduceSum
+ *   at the end:    VarAllGpuToCpu, FieldsWriteVtu
+ *
+ * Differences a caller can see, all deliberate:
+ *   - errors are returned (nonzero int, NULL pointer or NaN) with a message in
+ *     gbGetLastError(), where the reference prints and exit()s;
+ *   - C has no references, so `const vector&` / `const scalar&` arguments are
+ *     passed by value (gb_vector is layout-compatible with CUDA's float3);
+ *   - the device layout is private: cuMesh._hgpu/_gpu and FvmField._hgpu/_gpu
+ *     are NULL.  The host mirrors (_cpu) keep the reference's layout and the
+ *     reference's cell order, so code that reads mesh->_cpu or field->_cpu
+ *     after VarGpuToCpu sees what the reference would show;
+ *   - FvmEulerStep updates the state as a Jacobi sweep (every cell reads the
+ *     old state); the reference updates in place while neighbours read, a
+ *     race with the same fixed point.
+ *   - everything runs on the stream set with gbSetStream (default: the
+ *     legacy default stream, as in the reference).
+ *
+ * Additions that have no reference counterpart carry the gb prefix.
+ */
+#ifndef GRAPHITE_B200_H
+#define GRAPHITE_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* include/datatypes.cuh:36-47 (FLOAT_PREC build): scalar = float,
+ * vector = float3, tensor = three float3 columns (include/datatypes.cuh:52-54). */
+typedef float gb_scalar;
+typedef struct gb_vector { float x, y, z; } gb_vector;
+typedef struct gb_tensor { gb_vector u, v, w; } gb_tensor;
+
+/* include/mesh.cuh:12-16 */
+typedef enum CUMESH_t { _CPU, _HGPU, _GPU } CUMESH_t;
+
+/* Host mirror of a mesh, field for field as include/mesh.cuh:18-52, in the
+ * reference's cell order (elements in file order, then one ghost cell per
+ * boundary face, grouped by region).  Metrics are the float32 rounding of
+ * float64 values computed on the device. */
+typedef struct cuMeshBase {
+    CUMESH_t type;
+    int allocated;
+    size_t n_cells, n_faces, n_nodes, n_ghosts, n_regions;
+    unsigned int* cell_faces;
+    unsigned int* cell_connects;
+    unsigned int* cell_faces_starts;
+    gb_scalar* cell_volumes;
+    gb_vector* cell_centers;
+    gb_tensor* cell_matrices;
+    unsigned int* face_nodes;
+    unsigned int* face_nodes_starts;
+    gb_scalar* face_areas;
+    gb_vector* face_centers;
+    gb_vector* face_normals;
+    gb_vector* nodes;
+    unsigned int* ghost_cell_ids;
+    unsigned int* ghost_cell_starts;
+} cuMeshBase;
+
+/* include/mesh.cuh:55-63, plus a private pointer to the device mesh. */
+typedef struct cuMesh {
+    cuMeshBase* _cpu;
+    cuMeshBase* _hgpu; /* NULL: the device layout is private */
+    cuMeshBase* _gpu;  /* NULL */
+    char** region_names;
+    size_t region_names_alloc;
+    size_t region_names_size;
+    void* impl;
+} cuMesh;
+
+/* include/fvmfields.cuh:8-13 */
+typedef enum FvmFieldType { SCALAR, VECTOR, TENSOR, FIELD_UNKNOWN } FvmFieldType;
+
+/* include/fvmfields.cuh:16-22: value[size], gradient[3*size] and
+ * limiter[size] in element units (vector fields: gradient is a tensor whose
+ * columns are the gradients of x, y and z). */
+typedef struct FvmFieldBase {
+    size_t elem_size;
+    size_t size;
+    void* value;
+    void* gradient;
+    void* limiter;
+} FvmFieldBase;
+
+/* include/fvmfields.cuh:25-30, plus a private pointer to the device field. */
+typedef struct FvmField {
+    FvmFieldBase* _cpu;
+    FvmFieldBase* _hgpu; /* NULL: the device layout is private */
+    FvmFieldBase* _gpu;  /* NULL */
+    char* name;
+    void* impl;
+} FvmField;
+
+/* ---------------------------------------------------------------- mesh --- */
+
+/* Converts an SU2 text mesh (3-D; element kinds 10 tet, 12 hex, 13 prism,
+ * 14 pyramid; boundary kinds 5 triangle, 9 quad) to the binary .fvm format.
+ * Replaces cuMeshFromSu2, src/meshio.cu:817-1250 (same file layout; same
+ * cell, ghost and per-cell face order; faces are numbered in order of first
+ * appearance instead of hash-bucket order).  Returns 0 on success. */
+int cuMeshFromSu2(const char* su2_filename, const char* out_filename);
+
+/* Reads a .fvm mesh, renumbers cells (reverse Cuthill-McKee) and faces for
+ * locality, computes the metrics in float64 on the device and fills the host
+ * mirror.  Replaces cuMeshFromFile, src/meshio.cu:166-292 (and the metric
+ * kernels src/mesh.cu:44-219 it launches).  NULL on error. */
+cuMesh* cuMeshFromFile(const char* filename);
+
+/* Frees host and device memory.  Replaces cuMeshFree, src/mesh.cu:401-411. */
+void cuMeshFree(cuMesh* mesh);
+
+/* Size queries, src/mesh.cu:5-31. */
+size_t cuMeshGetVarSize(cuMesh* mesh);          /* cells + ghosts */
+size_t cuMeshGetnCells(cuMesh* mesh);
+size_t cuMeshGetnGhosts(cuMesh* mesh);
+size_t cuMeshGetnCellsAndGhosts(cuMesh* mesh);
+size_t cuMeshGetnRegionCells(cuMesh* mesh, unsigned int region_id);
+
+/* Region index by name, src/mesh.cu:17-23.  The reference prints and returns
+ * 0 for an unknown name; this returns UINT32_MAX and sets the last error. */
+unsigned int cuMeshGetRegionId(cuMesh* mesh, const char* name);
+
+/* Prints the mesh sizes, src/meshio.cu:8-21. */
+void cuMeshPrintInfo(cuMesh* mesh);
+
+/* -------------------------------------------------------------- fields --- */
+
+/* A field of `size` elements of `elem_size` bytes (sizeof(gb_scalar) or
+ * sizeof(gb_vector)), with gradient and limiter storage when alloc_grads is
+ * nonzero.  Replaces FvmFieldNew, src/fvmfields.cu:7-46.  The device storage
+ * takes the mesh's cell order the first time the field is used with a mesh.
+ * NULL on error. */
+FvmField* FvmFieldNew(size_t elem_size, size_t size, const char* name, int alloc_grads);
+
+/* src/fvmfields.cu:49-64 */
+void FvmFieldFree(FvmField* v);
+
+/* src/fvmfields.cu:67-83 */
+FvmFieldType FvmFieldGetType(const FvmField* v);
+void* FvmFieldValueIndex(FvmField* v, size_t i);
+
+/* Copies the values (VarGpuToCpu) or values, gradients and limiters
+ * (VarAllGpuToCpu) to field->_cpu in the reference's layout and cell order.
+ * Ghost gradients/limiters are those of the ghost's interior cell, as the
+ * reference's fvmScalGradLimBc/fvmVecGradLimBc leave them.  Synchronises the
+ * stream.  src/fvmfields.cu:85-101. */
+void VarGpuToCpu(FvmField* var);
+void VarAllGpuToCpu(FvmField* var);
+
+/* ----------------------------------------------------------- euler ops --- */
+
+/* Uniform state from Mach vector, pressure and temperature in cells and
+ * ghosts (gamma = 1.4, R = 1).  src/models/euler.cu:385-409, 529-549. */
+int FvmEulerInit(cuMesh* mesh, FvmField* rho, FvmField* rhou, FvmField* rhoe, gb_vector mach,
+                 gb_scalar pressure, gb_scalar temperature);
+
+/* Slip wall on a region's ghosts: mirrored momentum, copied density and
+ * energy.  src/models/euler.cu:412-442, 552-568. */
+int FvmEulerSlipBc(cuMesh* mesh, FvmField* rho, FvmField* rhou, FvmField* rhoe, const char* region);
+
+/* Far-field ghosts (sub/supersonic inflow/outflow from the interior Mach
+ * number and the sign of u.n).  src/models/euler.cu:446-520, 571-593. */
+int FvmEulerInletOutletBc(cuMesh* mesh, FvmField* rho, FvmField* rhou, FvmField* rhoe, gb_vector mach,
+                          gb_scalar pressure, gb_scalar temperature, const char* region);
+
+/* Least-squares gradients and limiters of rho, rhou, rhoe (one fused kernel).
+ * src/models/euler.cu:597-647 (9 kernels there). */
+int FvmEulerStepPrepare(cuMesh* mesh, FvmField* rho, FvmField* rhou, FvmField* rhoe);
+
+/* One local-time-step explicit update: reconstruction, central flux with
+ * scalar dissipation, dt = cfl / sum(eig * A / V), and the squared residual
+ * (F_rho^2 + |F_rhou|^2 + F_rhoE^2) * V into `error` (one fused kernel).
+ * time_scheme must be "steady"; dt is unused (NULL), as in the reference.
+ * src/models/euler.cu:236-381, 649-673. */
+int FvmEulerStep(cuMesh* mesh, FvmField* rho, FvmField* rhou, FvmField* rhoe, gb_scalar cfl,
+                 const char* time_scheme, FvmField* dt, FvmField* error);
+
+/* Sum of a scalar field over the interior cells, accumulated in float64 on
+ * the device in a fixed order (the result is deterministic) and returned
+ * rounded to float.  Replaces FvmFieldReduceSum, src/fvmops.cu:369-383, which
+ * copies the field to the host and sums it serially in float.  NaN on error. */
+gb_scalar FvmFieldReduceSum(cuMesh* mesh, FvmField* var);
+
+/* ----------------------------------------------------------- additions --- */
+
+/* Message of the last error on this thread ("" if none). */
+const char* gbGetLastError(void);
+
+/* Stream for all subsequent work of this library on this thread (a
+ * cudaStream_t; NULL = legacy default stream). */
+int gbSetStream(void* stream);
+void* gbGetStream(void);
+
+/* Copies field->_cpu->value (reference layout and order) to the device; the
+ * reverse of VarGpuToCpu, which the reference does not have.  Needs a field
+ * already bound to `mesh`'s cell order (used with the mesh once) or binds
+ * it now. */
+int gbVarCpuToGpu(cuMesh* mesh, FvmField* var);
+
+/* Momentum reconstruction: 1 (default) reproduces the reference, which
+ * reconstructs rhou with the transposed gradient (dot(tensor, d) is a column
+ * combination, include/datatypes.cuh:296-302, used at
+ * src/models/euler.cu:252-253); 0 uses the consistent gradient. */
+int gbSetReferenceMomentumReconstruction(int enabled);
+
+/* Cell renumbering applied by cuMeshFromFile / gbMeshFromSu2: 1 (default)
+ * reverse Cuthill-McKee, 0 keeps the file order. */
+int gbSetRenumbering(int enabled);
+
+/* Loads an SU2 mesh directly (no .fvm round trip; node coordinates stay
+ * float64).  NULL on error. */
+cuMesh* gbMeshFromSu2(const char* su2_filename);
+
+/* Boundary condition for gbEulerRun: type 0 slip, 1 far field (mach,
+ * pressure, temperature used). */
+typedef struct gbBc {
+    int type;
+    unsigned int region_id;
+    gb_vector mach;
+    gb_scalar pressure;
+    gb_scalar temperature;
+} gbBc;
+
+/* Runs n_iter iterations of the PhysicsEuler::step loop (boundary conditions
+ * in the given order, prepare, step, residual sum) as a replayed CUDA graph,
+ * writing the residual sum of each iteration to residual_history (host
+ * array of n_iter doubles, may be NULL).  Stops early, after the iteration
+ * in which residual/residual[0] < tolerance, when tolerance > 0 (checked
+ * every check_every iterations; the residuals between checks are still
+ * recorded).  Returns the number of iterations run, or -1 on error. */
+int64_t gbEulerRun(cuMesh* mesh, FvmField* rho, FvmField* rhou, FvmField* rhoe, FvmField* error,
+                   gb_scalar cfl, int64_t n_iter, const gbBc* bcs, int n_bc, double tolerance,
+                   int check_every, double* residual_history);
+
+/* Launches of this library's kernels since load (for accounting). */
+uint64_t gbKernelLaunchCount(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* GRAPHITE_B200_H */

@@ -1,0 +1,122 @@
+"""Generate the golden fixtures by running the reference solver itself.
+
+Needs a GPU and the headless reference build (``make -f oracle/Makefile.ref``
+in a tree where the reference sources are present; the built
+``oracle/_ref/ref_driver`` then runs anywhere with the same CUDA runtime).
+
+    python tests/golden/make_golden.py --out tests/golden
+
+For each case in cases.py it writes the SU2 mesh, runs the driver in one of
+its modes and stores the arrays as ``<case>_<mode>.npz``:
+
+* metrics  - the reference's mesh arrays after cuMeshFromSu2/cuMeshFromFile
+             (CSR topology, face areas/normals/centres, cell volumes/centres,
+             inverse LSQ matrices), for every element kind;
+* prepare  - value/gradient/limiter of rho, rhou, rhoe after the boundary
+             conditions and FvmEulerStepPrepare, from a seeded synthetic state;
+* solve    - residual history and final fields after a fixed number of
+             PhysicsEuler::step iterations from the uniform freestream.
+"""
+from __future__ import annotations
+
+import argparse
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, HERE)
+
+import cases  # noqa: E402
+import refio  # noqa: E402
+
+DRIVER = os.path.join(ROOT, "oracle", "_ref", "ref_driver")
+
+METRICS = ["tet_6x3x2", "hex_6x3x2", "prism_6x3x2", "pyramid_6x3x2", "tet_12x6x2"]
+PREPARE = ["tet_6x3x2", "hex_6x3x2", "prism_6x3x2", "pyramid_6x3x2", "tet_12x6x2"]
+SOLVES = [("tet_12x6x2", 20000), ("channel", 2000), ("channel", 40000)]
+
+FLOAT_KEYS_METRICS = ["nodes", "face_areas", "face_normals", "face_centers", "cell_volumes",
+                      "cell_centers", "cell_matrices"]
+INT_KEYS_METRICS = ["cell_faces_starts", "cell_faces", "cell_connects", "face_nodes_starts", "face_nodes",
+                    "ghost_cell_ids", "ghost_cell_starts"]
+
+
+def run(args, log):
+    t = time.time()
+    r = subprocess.run(args, stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True)
+    log.write(" ".join(args) + f"\n  -> rc={r.returncode} {time.time() - t:.1f}s\n" + r.stdout[-2000:] + "\n")
+    log.flush()
+    if r.returncode != 0:
+        raise SystemExit(f"driver failed: {' '.join(args)}\n{r.stdout[-2000:]}")
+    return r.stdout
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--out", default=HERE)
+    ap.add_argument("--work", default=os.path.join(ROOT, "gpurun_out", "golden_work"))
+    ap.add_argument("--only", default="", help="comma list of metrics,prepare,solve")
+    a = ap.parse_args()
+    os.makedirs(a.out, exist_ok=True)
+    os.makedirs(a.work, exist_ok=True)
+    only = set(a.only.split(",")) if a.only else {"metrics", "prepare", "solve"}
+    log = open(os.path.join(a.work, "make_golden.log"), "a")
+    meshes = {}
+
+    def su2(name):
+        if name not in meshes:
+            m = cases.MESHES[name]()
+            path = os.path.join(a.work, f"{name}.su2")
+            m.write_su2(path)
+            meshes[name] = (m, path)
+        return meshes[name]
+
+    init = cases.CHANNEL_MACH + (cases.P_INF, cases.T_INF)
+    bcs = cases.channel_bcs()
+    if "metrics" in only:
+        for name in METRICS:
+            m, path = su2(name)
+            case = os.path.join(a.work, f"{name}_metrics.txt")
+            refio.write_case(case, init, bcs)
+            out = os.path.join(a.work, f"{name}_metrics.bin")
+            run([DRIVER, case, path, out, "metrics"], log)
+            rec = refio.read_records(out)
+            np.savez_compressed(os.path.join(a.out, f"{name}_metrics.npz"), sizes=rec["sizes"],
+                                **{k: rec[k] for k in FLOAT_KEYS_METRICS + INT_KEYS_METRICS})
+    if "prepare" in only:
+        for name in PREPARE:
+            m, path = su2(name)
+            rho, rhou, rhoe = cases.synthetic_state(m)
+            state = os.path.join(a.work, f"{name}_state.bin")
+            np.concatenate([rho, rhou.reshape(-1), rhoe]).astype(np.float32).tofile(state)
+            case = os.path.join(a.work, f"{name}_prepare.txt")
+            refio.write_case(case, init, bcs, state=state)
+            out = os.path.join(a.work, f"{name}_prepare.bin")
+            run([DRIVER, case, path, out, "prepare"], log)
+            rec = refio.read_records(out)
+            keep = {k: v for k, v in rec.items() if k.split(".")[0] in ("rho", "rhou", "rhoe")}
+            np.savez_compressed(os.path.join(a.out, f"{name}_prepare.npz"), sizes=rec["sizes"],
+                                state_rho=rho, state_rhou=rhou, state_rhoe=rhoe, **keep)
+    if "solve" in only:
+        for name, iters in SOLVES:
+            m, path = su2(name)
+            case = os.path.join(a.work, f"{name}_solve{iters}.txt")
+            refio.write_case(case, init, bcs, cfl=0.8, iters=iters)
+            out = os.path.join(a.work, f"{name}_solve{iters}.bin")
+            txt = run([DRIVER, case, path, out, "solve"], log)
+            rec = refio.read_records(out)
+            keep = {k: rec[k] for k in ("rho.value", "rhou.value", "rhoe.value", "residual_history",
+                                        "iterations", "wall_seconds", "event_seconds", "sizes")}
+            np.savez_compressed(os.path.join(a.out, f"{name}_solve{iters}.npz"), **keep)
+            print(name, iters, txt.strip().splitlines()[-1])
+    log.close()
+
+
+if __name__ == "__main__":
+    main()
