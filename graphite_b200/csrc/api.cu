@@ -1,0 +1,749 @@
+// extern "C" entry points of libgraphite_b200.so (see include/graphite_b200.h).
+#include <atomic>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <limits>
+#include <string>
+#include <vector>
+
+#include "gb_device.cuh"
+#include "gb_internal.h"
+
+namespace gb {
+
+namespace {
+thread_local std::string t_error;
+thread_local cudaStream_t t_stream = nullptr;
+std::atomic<uint64_t> g_launches{0};
+std::atomic<int> g_transposed{1};
+std::atomic<int> g_renumber{1};
+thread_local bool t_counting = true;
+}  // namespace
+
+void set_error(const std::string& msg) { t_error = msg; }
+void clear_error() { t_error.clear(); }
+void count_launch(int n) {
+    if (t_counting) g_launches += (uint64_t)n;
+}
+
+namespace {
+
+bool cuda_ok(cudaError_t e, const char* what) {
+    if (e == cudaSuccess) return true;
+    set_error(std::string(what) + ": " + cudaGetErrorString(e));
+    return false;
+}
+
+bool launch_ok(const char* what) { return cuda_ok(cudaGetLastError(), what); }
+
+template <typename T>
+bool dalloc(T*& p, size_t n, const char* what) {
+    p = nullptr;
+    if (n == 0) return true;
+    return cuda_ok(cudaMalloc((void**)&p, n * sizeof(T)), what);
+}
+
+template <typename T>
+bool upload(T*& p, const std::vector<T>& v, const char* what) {
+    if (!dalloc(p, v.size(), what)) return false;
+    if (v.empty()) return true;
+    return cuda_ok(cudaMemcpyAsync(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, t_stream), what);
+}
+
+template <typename T>
+void dfree(T*& p) {
+    if (p) cudaFree((void*)p);
+    p = nullptr;
+}
+
+struct MeshImpl {
+    Topology topo;
+    Numbering num;
+    DevMesh dev;
+    uint32_t* d_cell_new = nullptr;   // old -> new, N+G
+};
+
+struct FieldImpl {
+    int comps = 1;                    // 1 scalar, 3 vector
+    size_t size = 0;
+    int alloc_grads = 0;
+    void* val[2] = {nullptr, nullptr};   // float* or float4*
+    int cur = 0;
+    float4* grad = nullptr;           // N (scalar) or 3N (vector), bound mesh order
+    const cuMesh* bound = nullptr;
+    double* partials = nullptr;
+    int n_partials = 0;
+    bool partials_valid = false;
+    float* staging = nullptr;         // size * comps floats
+};
+
+MeshImpl* impl(cuMesh* m) { return m ? static_cast<MeshImpl*>(m->impl) : nullptr; }
+FieldImpl* impl(const FvmField* f) { return f ? static_cast<FieldImpl*>(f->impl) : nullptr; }
+
+template <typename T>
+T* hmalloc(size_t n) {
+    return static_cast<T*>(calloc(n ? n : 1, sizeof(T)));
+}
+
+void free_host_mesh(cuMeshBase* b) {
+    if (!b) return;
+    free(b->cell_faces); free(b->cell_connects); free(b->cell_faces_starts);
+    free(b->cell_volumes); free(b->cell_centers); free(b->cell_matrices);
+    free(b->face_nodes); free(b->face_nodes_starts); free(b->face_areas);
+    free(b->face_centers); free(b->face_normals); free(b->nodes);
+    free(b->ghost_cell_ids); free(b->ghost_cell_starts);
+    free(b);
+}
+
+void free_mesh(cuMesh* m) {
+    if (!m) return;
+    MeshImpl* mi = impl(m);
+    if (mi) {
+        DevMesh& d = mi->dev;
+        dfree(d.cell_geo); dfree(d.face_geo); dfree(d.start); dfree(d.nb); dfree(d.lsq); dfree(d.ghost); dfree(d.red);
+        dfree(mi->d_cell_new);
+        delete mi;
+    }
+    free_host_mesh(m->_cpu);
+    for (size_t i = 0; i < m->region_names_size; ++i) free(m->region_names[i]);
+    free(m->region_names);
+    free(m);
+}
+
+// Topology -> device mesh + host mirror.
+cuMesh* create_mesh(Topology&& topo) {
+    cudaStream_t s = t_stream;
+    cuMesh* m = hmalloc<cuMesh>(1);
+    MeshImpl* mi = new MeshImpl();
+    m->impl = mi;
+    mi->topo = std::move(topo);
+    const Topology& t = mi->topo;
+    const int64_t N = t.N, G = t.G, NG = N + G, F = t.F;
+    number_cells(t, g_renumber.load() != 0, mi->num);
+    const Numbering& num = mi->num;
+    DevMesh& d = mi->dev;
+    d.N = N; d.G = G; d.F = F; d.S = (int64_t)num.nb_face.size();
+
+    // float64 metrics in the reference's order
+    double *d_nodes = nullptr, *area = nullptr, *normal = nullptr, *fcen = nullptr, *ccen = nullptr, *vol = nullptr,
+           *minv = nullptr;
+    uint32_t *d_fns = nullptr, *d_fn = nullptr, *d_cfs = nullptr, *d_cf = nullptr, *d_cc = nullptr,
+             *d_cell_old = nullptr, *d_face_old = nullptr;
+    bool ok = upload(d_nodes, t.nodes, "upload nodes") && upload(d_fns, t.fns, "upload face nodes") &&
+              upload(d_fn, t.fn, "upload face nodes") && upload(d_cfs, t.cfs, "upload cells") &&
+              upload(d_cf, t.cf, "upload cells") && upload(d_cc, t.cc, "upload cells") &&
+              dalloc(area, F, "alloc metrics") && dalloc(normal, 3 * F, "alloc metrics") &&
+              dalloc(fcen, 3 * F, "alloc metrics") && dalloc(ccen, 3 * NG, "alloc metrics") &&
+              dalloc(vol, NG, "alloc metrics") && dalloc(minv, 9 * N, "alloc metrics");
+    if (ok) {
+        launch_face_metrics64(F, d_nodes, d_fns, d_fn, area, normal, fcen, s);
+        launch_cell_metrics64(N, d_cfs, d_cf, area, normal, fcen, ccen, vol, s);
+        launch_ghost_metrics64(G, N, d_cfs, d_cf, d_cc, area, normal, fcen, ccen, vol, s);
+        launch_lsq64(N, d_cfs, d_cc, ccen, minv, s);
+        ok = launch_ok("metric kernels");
+    }
+    // renumbered float32 layout
+    std::vector<uint2> nb(d.S), gl(G);
+    for (int64_t k = 0; k < d.S; ++k) nb[k] = make_uint2(num.nb_face[k], num.nb_cell[k]);
+    for (int64_t g = 0; g < G; ++g) gl[g] = make_uint2(num.ghost_cell[g], num.ghost_face[g]);
+    ok = ok && upload(d_cell_old, num.cell_old, "upload numbering") && upload(d_face_old, num.face_old, "upload numbering") &&
+         upload(mi->d_cell_new, num.cell_new, "upload numbering") && dalloc(d.cell_geo, NG, "alloc mesh") &&
+         dalloc(d.face_geo, 2 * F, "alloc mesh") && upload(d.start, num.start, "upload csr") &&
+         upload(d.nb, nb, "upload csr") && dalloc(d.lsq, 2 * N, "alloc mesh") && upload(d.ghost, gl, "upload ghosts");
+    d.n_red_max = std::max<int>(reduce_blocks(NG), (int)((N + kBlock - 1) / kBlock));
+    ok = ok && dalloc(d.red, (size_t)d.n_red_max + 1, "alloc reduction");
+    if (ok) {
+        launch_layout(d, d_cell_old, d_face_old, area, normal, fcen, ccen, vol, minv, s);
+        ok = launch_ok("layout kernels");
+    }
+    // host mirror in the reference's layout and order
+    cuMeshBase* b = hmalloc<cuMeshBase>(1);
+    m->_cpu = b;
+    b->type = _CPU;
+    b->allocated = 1;
+    b->n_cells = N; b->n_faces = F; b->n_nodes = t.nodes.size() / 3; b->n_ghosts = G; b->n_regions = t.regions.size();
+    if (ok) {
+        std::vector<double> h_area(F), h_normal(3 * F), h_fcen(3 * F), h_ccen(3 * NG), h_vol(NG), h_minv(9 * N);
+        ok = cuda_ok(cudaMemcpyAsync(h_area.data(), area, F * 8, cudaMemcpyDeviceToHost, s), "download metrics") &&
+             cuda_ok(cudaMemcpyAsync(h_normal.data(), normal, 3 * F * 8, cudaMemcpyDeviceToHost, s), "download metrics") &&
+             cuda_ok(cudaMemcpyAsync(h_fcen.data(), fcen, 3 * F * 8, cudaMemcpyDeviceToHost, s), "download metrics") &&
+             cuda_ok(cudaMemcpyAsync(h_ccen.data(), ccen, 3 * NG * 8, cudaMemcpyDeviceToHost, s), "download metrics") &&
+             cuda_ok(cudaMemcpyAsync(h_vol.data(), vol, NG * 8, cudaMemcpyDeviceToHost, s), "download metrics") &&
+             cuda_ok(cudaMemcpyAsync(h_minv.data(), minv, 9 * N * 8, cudaMemcpyDeviceToHost, s), "download metrics") &&
+             cuda_ok(cudaStreamSynchronize(s), "mesh setup");
+        if (ok) {
+            auto cpy_u32 = [](const std::vector<uint32_t>& v) {
+                unsigned* p = hmalloc<unsigned>(v.size());
+                if (!v.empty()) memcpy(p, v.data(), v.size() * 4);
+                return p;
+            };
+            b->cell_faces = cpy_u32(t.cf); b->cell_connects = cpy_u32(t.cc); b->cell_faces_starts = cpy_u32(t.cfs);
+            b->face_nodes = cpy_u32(t.fn); b->face_nodes_starts = cpy_u32(t.fns);
+            b->ghost_cell_ids = cpy_u32(t.ghost_ids); b->ghost_cell_starts = cpy_u32(t.ghost_starts);
+            b->cell_volumes = hmalloc<float>(NG);
+            b->cell_centers = hmalloc<gb_vector>(NG);
+            b->cell_matrices = hmalloc<gb_tensor>(N);
+            b->face_areas = hmalloc<float>(F);
+            b->face_centers = hmalloc<gb_vector>(F);
+            b->face_normals = hmalloc<gb_vector>(F);
+            b->nodes = hmalloc<gb_vector>(b->n_nodes);
+            for (int64_t i = 0; i < NG; ++i) {
+                b->cell_volumes[i] = (float)h_vol[i];
+                b->cell_centers[i] = {(float)h_ccen[3 * i], (float)h_ccen[3 * i + 1], (float)h_ccen[3 * i + 2]};
+            }
+            for (int64_t i = 0; i < N; ++i) {
+                float* p = &b->cell_matrices[i].u.x;
+                for (int k = 0; k < 9; ++k) p[k] = (float)h_minv[9 * i + k];
+            }
+            for (int64_t f = 0; f < F; ++f) {
+                b->face_areas[f] = (float)h_area[f];
+                b->face_centers[f] = {(float)h_fcen[3 * f], (float)h_fcen[3 * f + 1], (float)h_fcen[3 * f + 2]};
+                b->face_normals[f] = {(float)h_normal[3 * f], (float)h_normal[3 * f + 1], (float)h_normal[3 * f + 2]};
+            }
+            for (size_t i = 0; i < b->n_nodes; ++i)
+                b->nodes[i] = {(float)t.nodes[3 * i], (float)t.nodes[3 * i + 1], (float)t.nodes[3 * i + 2]};
+        }
+    }
+    dfree(d_nodes); dfree(area); dfree(normal); dfree(fcen); dfree(ccen); dfree(vol); dfree(minv);
+    dfree(d_fns); dfree(d_fn); dfree(d_cfs); dfree(d_cf); dfree(d_cc); dfree(d_cell_old); dfree(d_face_old);
+    m->region_names_alloc = m->region_names_size = t.regions.size();
+    m->region_names = hmalloc<char*>(t.regions.size());
+    for (size_t r = 0; r < t.regions.size(); ++r) m->region_names[r] = strdup(t.regions[r].c_str());
+    if (!ok) {
+        free_mesh(m);
+        return nullptr;
+    }
+    return m;
+}
+
+bool check_mesh(cuMesh* m) {
+    if (!m || !impl(m)) { set_error("null mesh"); return false; }
+    return true;
+}
+
+// Binds a field's device storage to a mesh's cell order (first use).
+bool bind(cuMesh* mesh, FvmField* f, int comps, const char* what) {
+    FieldImpl* fi = impl(f);
+    if (!fi) { set_error(std::string(what) + ": null field"); return false; }
+    if (fi->comps != comps) {
+        set_error(std::string(what) + ": field '" + f->name + (comps == 1 ? "' must be a scalar field" : "' must be a vector field"));
+        return false;
+    }
+    const MeshImpl* mi = impl(mesh);
+    if ((int64_t)fi->size != mi->topo.N + mi->topo.G) {
+        set_error(std::string(what) + ": field '" + f->name + "' has " + std::to_string(fi->size) +
+                  " elements, the mesh has " + std::to_string(mi->topo.N + mi->topo.G) + " cells and ghosts");
+        return false;
+    }
+    if (fi->bound && fi->bound != mesh) {
+        set_error(std::string(what) + ": field '" + f->name + "' is already used with another mesh");
+        return false;
+    }
+    fi->bound = mesh;
+    return true;
+}
+
+bool ensure_grad(cuMesh* mesh, FvmField* f) {
+    FieldImpl* fi = impl(f);
+    if (fi->grad) return true;
+    const int64_t N = impl(mesh)->topo.N;
+    if (!dalloc(fi->grad, (size_t)N * fi->comps, "alloc gradient")) return false;
+    return cuda_ok(cudaMemsetAsync(fi->grad, 0, (size_t)N * fi->comps * sizeof(float4), t_stream), "zero gradient");
+}
+
+bool ensure_partials(FieldImpl* fi, int n) {
+    if (fi->n_partials >= n) return true;
+    dfree(fi->partials);
+    fi->n_partials = 0;
+    if (!dalloc(fi->partials, (size_t)n, "alloc partials")) return false;
+    fi->n_partials = n;
+    return true;
+}
+
+bool ensure_staging(FieldImpl* fi) {
+    if (fi->staging) return true;
+    return dalloc(fi->staging, fi->size * fi->comps, "alloc staging");
+}
+
+bool euler_fields(cuMesh* mesh, FvmField* rho, FvmField* rhou, FvmField* rhoe, const char* what) {
+    if (!check_mesh(mesh)) return false;
+    if (!bind(mesh, rho, 1, what) || !bind(mesh, rhou, 3, what) || !bind(mesh, rhoe, 1, what)) return false;
+    FieldImpl *a = impl(rho), *b = impl(rhou), *c = impl(rhoe);
+    if (a->cur != b->cur || a->cur != c->cur) {
+        set_error(std::string(what) + ": rho, rhou and rhoe were not updated together");
+        return false;
+    }
+    return true;
+}
+
+EulerState state_of(FvmField* rho, FvmField* rhou, FvmField* rhoe, int buf) {
+    return EulerState{(const float*)impl(rho)->val[buf], (const float4*)impl(rhou)->val[buf],
+                      (const float*)impl(rhoe)->val[buf]};
+}
+
+int region_lookup(cuMesh* mesh, const char* region) {
+    const Topology& t = impl(mesh)->topo;
+    if (!region) { set_error("null region name"); return -1; }
+    for (size_t r = 0; r < t.regions.size(); ++r)
+        if (t.regions[r] == region) return (int)r;
+    set_error(std::string("region with name ") + region + " not found in mesh");
+    return -1;
+}
+
+void enqueue_slip(cuMesh* mesh, FvmField* rho, FvmField* rhou, FvmField* rhoe, int r, int cur, cudaStream_t s) {
+    MeshImpl* mi = impl(mesh);
+    float* pr[2] = {(float*)impl(rho)->val[0], (float*)impl(rho)->val[1]};
+    float4* pu[2] = {(float4*)impl(rhou)->val[0], (float4*)impl(rhou)->val[1]};
+    float* pe[2] = {(float*)impl(rhoe)->val[0], (float*)impl(rhoe)->val[1]};
+    launch_bc_slip(mi->dev, mi->num.region_start[r], mi->num.region_start[r + 1], pr, pu, pe, cur, s);
+}
+
+void enqueue_farfield(cuMesh* mesh, FvmField* rho, FvmField* rhou, FvmField* rhoe, int r, int cur, gb_vector mach,
+                      float p, float t, cudaStream_t s) {
+    MeshImpl* mi = impl(mesh);
+    float* pr[2] = {(float*)impl(rho)->val[0], (float*)impl(rho)->val[1]};
+    float4* pu[2] = {(float4*)impl(rhou)->val[0], (float4*)impl(rhou)->val[1]};
+    float* pe[2] = {(float*)impl(rhoe)->val[0], (float*)impl(rhoe)->val[1]};
+    launch_bc_farfield(mi->dev, mi->num.region_start[r], mi->num.region_start[r + 1], pr, pu, pe, cur,
+                       make_float3(mach.x, mach.y, mach.z), p, t, s);
+}
+
+EulerGrad grad_of(FvmField* rho, FvmField* rhou, FvmField* rhoe) {
+    return EulerGrad{impl(rho)->grad, impl(rhou)->grad, impl(rhoe)->grad};
+}
+
+void enqueue_flux(cuMesh* mesh, FvmField* rho, FvmField* rhou, FvmField* rhoe, FvmField* error, float cfl, int cur,
+                  cudaStream_t s) {
+    MeshImpl* mi = impl(mesh);
+    const int nxt = 1 - cur;
+    FieldImpl* ei = impl(error);
+    launch_flux(mi->dev, state_of(rho, rhou, rhoe, cur), grad_of(rho, rhou, rhoe), (float*)impl(rho)->val[nxt],
+                (float4*)impl(rhou)->val[nxt], (float*)impl(rhoe)->val[nxt], (float*)ei->val[ei->cur], ei->partials,
+                cfl, g_transposed.load() != 0, s);
+}
+
+// Reference-order host copy of the current values.
+bool download_values(FvmField* f) {
+    FieldImpl* fi = impl(f);
+    cudaStream_t s = t_stream;
+    const size_t bytes = fi->size * fi->comps * sizeof(float);
+    if (fi->size == 0) return true;
+    if (!fi->bound) {
+        // never used with a mesh: the device order is the caller's order
+        if (fi->comps == 1)
+            return cuda_ok(cudaMemcpyAsync(f->_cpu->value, fi->val[fi->cur], bytes, cudaMemcpyDeviceToHost, s), "copy field") &&
+                   cuda_ok(cudaStreamSynchronize(s), "copy field");
+        if (!ensure_staging(fi)) return false;
+        std::vector<float4> tmp(fi->size);
+        if (!cuda_ok(cudaMemcpyAsync(tmp.data(), fi->val[fi->cur], fi->size * 16, cudaMemcpyDeviceToHost, s), "copy field") ||
+            !cuda_ok(cudaStreamSynchronize(s), "copy field"))
+            return false;
+        float* h = (float*)f->_cpu->value;
+        for (size_t i = 0; i < fi->size; ++i) { h[3 * i] = tmp[i].x; h[3 * i + 1] = tmp[i].y; h[3 * i + 2] = tmp[i].z; }
+        return true;
+    }
+    if (!ensure_staging(fi)) return false;
+    const uint32_t* idx = impl(const_cast<cuMesh*>(fi->bound))->d_cell_new;
+    if (fi->comps == 1) launch_gather_scalar((int64_t)fi->size, (const float*)fi->val[fi->cur], idx, fi->staging, s);
+    else launch_gather_vector((int64_t)fi->size, (const float4*)fi->val[fi->cur], idx, fi->staging, s);
+    return launch_ok("gather field") &&
+           cuda_ok(cudaMemcpyAsync(f->_cpu->value, fi->staging, bytes, cudaMemcpyDeviceToHost, s), "copy field") &&
+           cuda_ok(cudaStreamSynchronize(s), "copy field");
+}
+
+bool download_gradients(FvmField* f) {
+    FieldImpl* fi = impl(f);
+    if (!fi->alloc_grads || !f->_cpu->gradient) return true;
+    const size_t n = fi->size;
+    float* hg = (float*)f->_cpu->gradient;   // 3 (scalar) or 9 (vector) floats per element
+    float* hl = (float*)f->_cpu->limiter;    // 1 or 3 floats per element
+    if (!fi->grad || !fi->bound) {
+        memset(hg, 0, n * fi->comps * 3 * sizeof(float));
+        for (size_t i = 0; i < n * fi->comps; ++i) hl[i] = 1.f;
+        return true;
+    }
+    const MeshImpl* mi = impl(const_cast<cuMesh*>(fi->bound));
+    const Topology& t = mi->topo;
+    const int64_t N = t.N;
+    std::vector<float4> g((size_t)N * fi->comps);
+    if (!cuda_ok(cudaMemcpyAsync(g.data(), fi->grad, g.size() * 16, cudaMemcpyDeviceToHost, t_stream), "copy gradient") ||
+        !cuda_ok(cudaStreamSynchronize(t_stream), "copy gradient"))
+        return false;
+    for (size_t o = 0; o < n; ++o) {
+        // ghosts carry their interior cell's gradient and limiter
+        const uint32_t src = (int64_t)o < N ? (uint32_t)o : t.cc[t.cfs[o]];
+        const uint32_t i = mi->num.cell_new[src];
+        for (int a = 0; a < fi->comps; ++a) {
+            const float4 v = g[(size_t)i * fi->comps + a];
+            hg[(o * fi->comps + a) * 3 + 0] = v.x;
+            hg[(o * fi->comps + a) * 3 + 1] = v.y;
+            hg[(o * fi->comps + a) * 3 + 2] = v.z;
+            hl[o * fi->comps + a] = v.w;
+        }
+    }
+    return true;
+}
+
+}  // namespace
+}  // namespace gb
+
+using namespace gb;
+
+extern "C" {
+
+const char* gbGetLastError(void) { return t_error.c_str(); }
+
+int gbSetStream(void* stream) {
+    t_stream = (cudaStream_t)stream;
+    return 0;
+}
+
+void* gbGetStream(void) { return (void*)t_stream; }
+
+uint64_t gbKernelLaunchCount(void) { return g_launches.load(); }
+
+int gbSetReferenceMomentumReconstruction(int enabled) {
+    g_transposed = enabled ? 1 : 0;
+    return 0;
+}
+
+int gbSetRenumbering(int enabled) {
+    g_renumber = enabled ? 1 : 0;
+    return 0;
+}
+
+int cuMeshFromSu2(const char* su2_filename, const char* out_filename) {
+    clear_error();
+    ElementSet es;
+    Topology t;
+    if (!su2_filename || !out_filename) { set_error("null file name"); return 1; }
+    if (!parse_su2(su2_filename, es) || !build_topology(es, t) || !write_fvm(out_filename, t)) return 1;
+    return 0;
+}
+
+cuMesh* cuMeshFromFile(const char* filename) {
+    clear_error();
+    Topology t;
+    if (!filename) { set_error("null file name"); return nullptr; }
+    if (!read_fvm(filename, t)) return nullptr;
+    return create_mesh(std::move(t));
+}
+
+cuMesh* gbMeshFromSu2(const char* su2_filename) {
+    clear_error();
+    ElementSet es;
+    Topology t;
+    if (!su2_filename) { set_error("null file name"); return nullptr; }
+    if (!parse_su2(su2_filename, es) || !build_topology(es, t)) return nullptr;
+    return create_mesh(std::move(t));
+}
+
+void cuMeshFree(cuMesh* mesh) { free_mesh(mesh); }
+
+size_t cuMeshGetVarSize(cuMesh* m) { return m ? m->_cpu->n_cells + m->_cpu->n_ghosts : 0; }
+size_t cuMeshGetnCells(cuMesh* m) { return m ? m->_cpu->n_cells : 0; }
+size_t cuMeshGetnGhosts(cuMesh* m) { return m ? m->_cpu->n_ghosts : 0; }
+size_t cuMeshGetnCellsAndGhosts(cuMesh* m) { return cuMeshGetVarSize(m); }
+
+size_t cuMeshGetnRegionCells(cuMesh* m, unsigned int r) {
+    if (!m || r >= m->_cpu->n_regions) return 0;
+    return m->_cpu->ghost_cell_starts[r + 1] - m->_cpu->ghost_cell_starts[r];
+}
+
+unsigned int cuMeshGetRegionId(cuMesh* m, const char* name) {
+    clear_error();
+    if (!check_mesh(m)) return UINT32_MAX;
+    const int r = region_lookup(m, name);
+    return r < 0 ? UINT32_MAX : (unsigned)r;
+}
+
+void cuMeshPrintInfo(cuMesh* m) {
+    if (!m) return;
+    const cuMeshBase* b = m->_cpu;
+    printf("Printing info on cuMesh object\n");
+    printf("- n_cells = %zu\n", b->n_cells);
+    printf("- n_faces = %zu\n", b->n_faces);
+    printf("- n_nodes = %zu\n", b->n_nodes);
+    printf("- n_ghosts = %zu\n", b->n_ghosts);
+    printf("- n_regions = %zu\n", b->n_regions);
+    printf("- n_cells_faces = %u\n", b->cell_faces_starts[b->n_cells + b->n_ghosts]);
+    printf("- n_face_nodes = %u\n", b->face_nodes_starts[b->n_faces]);
+    printf("- renumbering bandwidth = %lld\n", (long long)impl(m)->num.bandwidth);
+}
+
+FvmField* FvmFieldNew(size_t elem_size, size_t size, const char* name, int alloc_grads) {
+    clear_error();
+    int comps;
+    if (elem_size == sizeof(gb_scalar)) comps = 1;
+    else if (elem_size == sizeof(gb_vector)) comps = 3;
+    else { set_error("FvmFieldNew: elem_size must be sizeof(scalar) or sizeof(vector)"); return nullptr; }
+    FvmField* f = hmalloc<FvmField>(1);
+    FieldImpl* fi = new FieldImpl();
+    f->impl = fi;
+    f->name = strdup(name ? name : "");
+    fi->comps = comps;
+    fi->size = size;
+    fi->alloc_grads = alloc_grads;
+    f->_cpu = hmalloc<FvmFieldBase>(1);
+    f->_cpu->elem_size = elem_size;
+    f->_cpu->size = size;
+    f->_cpu->value = calloc(size ? size : 1, elem_size);
+    if (alloc_grads) {
+        f->_cpu->gradient = calloc(size ? size : 1, elem_size * 3);
+        f->_cpu->limiter = calloc(size ? size : 1, elem_size);
+    }
+    const size_t vb = comps == 1 ? sizeof(float) : sizeof(float4);
+    bool ok = true;
+    for (int k = 0; k < 2 && ok; ++k) {
+        ok = cuda_ok(cudaMalloc(&fi->val[k], (size ? size : 1) * vb), "FvmFieldNew") &&
+             cuda_ok(cudaMemsetAsync(fi->val[k], 0, (size ? size : 1) * vb, t_stream), "FvmFieldNew");
+    }
+    if (!ok) {
+        FvmFieldFree(f);
+        return nullptr;
+    }
+    return f;
+}
+
+void FvmFieldFree(FvmField* f) {
+    if (!f) return;
+    FieldImpl* fi = impl(f);
+    if (fi) {
+        dfree(fi->val[0]); dfree(fi->val[1]); dfree(fi->grad); dfree(fi->partials); dfree(fi->staging);
+        delete fi;
+    }
+    if (f->_cpu) {
+        free(f->_cpu->value); free(f->_cpu->gradient); free(f->_cpu->limiter);
+        free(f->_cpu);
+    }
+    free(f->name);
+    free(f);
+}
+
+FvmFieldType FvmFieldGetType(const FvmField* v) {
+    if (!v) return FIELD_UNKNOWN;
+    if (v->_cpu->elem_size == sizeof(gb_scalar)) return SCALAR;
+    if (v->_cpu->elem_size == sizeof(gb_vector)) return VECTOR;
+    if (v->_cpu->elem_size == sizeof(gb_tensor)) return TENSOR;
+    return FIELD_UNKNOWN;
+}
+
+void* FvmFieldValueIndex(FvmField* v, size_t i) {
+    return v ? (void*)((char*)v->_cpu->value + v->_cpu->elem_size * i) : nullptr;
+}
+
+void VarGpuToCpu(FvmField* var) {
+    clear_error();
+    if (var && impl(var)) download_values(var);
+}
+
+void VarAllGpuToCpu(FvmField* var) {
+    clear_error();
+    if (var && impl(var) && download_values(var)) download_gradients(var);
+}
+
+int gbVarCpuToGpu(cuMesh* mesh, FvmField* var) {
+    clear_error();
+    if (!check_mesh(mesh)) return 1;
+    FieldImpl* fi = impl(var);
+    if (!fi || !bind(mesh, var, fi->comps, "gbVarCpuToGpu") || !ensure_staging(fi)) return 1;
+    cudaStream_t s = t_stream;
+    const uint32_t* idx = impl(mesh)->d_cell_new;
+    if (!cuda_ok(cudaMemcpyAsync(fi->staging, var->_cpu->value, fi->size * fi->comps * 4, cudaMemcpyHostToDevice, s),
+                 "gbVarCpuToGpu"))
+        return 1;
+    for (int k = 0; k < 2; ++k) {
+        if (fi->comps == 1) launch_scatter_scalar((int64_t)fi->size, fi->staging, idx, (float*)fi->val[k], s);
+        else launch_scatter_vector((int64_t)fi->size, fi->staging, idx, (float4*)fi->val[k], s);
+    }
+    fi->partials_valid = false;
+    return launch_ok("gbVarCpuToGpu") ? 0 : 1;
+}
+
+int FvmEulerInit(cuMesh* mesh, FvmField* rho, FvmField* rhou, FvmField* rhoe, gb_vector mach, gb_scalar pressure,
+                 gb_scalar temperature) {
+    clear_error();
+    if (!check_mesh(mesh) || !bind(mesh, rho, 1, "FvmEulerInit") || !bind(mesh, rhou, 3, "FvmEulerInit") ||
+        !bind(mesh, rhoe, 1, "FvmEulerInit"))
+        return 1;
+    // euler_init, src/models/euler.cu:401-404
+    const float r = pressure / temperature;
+    const float c = sqrtf(1.4f * pressure / r);
+    const float3 vel = make_float3(mach.x * c, mach.y * c, mach.z * c);
+    const float3 ru = make_float3(vel.x * r, vel.y * r, vel.z * r);
+    const float e = pressure / 0.4f + 0.5f * r * (vel.x * vel.x + vel.y * vel.y + vel.z * vel.z);
+    const int64_t n = (int64_t)impl(rho)->size;
+    for (int k = 0; k < 2; ++k)
+        launch_init(n, (float*)impl(rho)->val[k], (float4*)impl(rhou)->val[k], (float*)impl(rhoe)->val[k], r, ru, e,
+                    t_stream);
+    impl(rho)->cur = impl(rhou)->cur = impl(rhoe)->cur = 0;
+    return launch_ok("FvmEulerInit") ? 0 : 1;
+}
+
+int FvmEulerSlipBc(cuMesh* mesh, FvmField* rho, FvmField* rhou, FvmField* rhoe, const char* region) {
+    clear_error();
+    if (!euler_fields(mesh, rho, rhou, rhoe, "FvmEulerSlipBc")) return 1;
+    const int r = region_lookup(mesh, region);
+    if (r < 0) return 1;
+    enqueue_slip(mesh, rho, rhou, rhoe, r, impl(rho)->cur, t_stream);
+    return launch_ok("FvmEulerSlipBc") ? 0 : 1;
+}
+
+int FvmEulerInletOutletBc(cuMesh* mesh, FvmField* rho, FvmField* rhou, FvmField* rhoe, gb_vector mach,
+                          gb_scalar pressure, gb_scalar temperature, const char* region) {
+    clear_error();
+    if (!euler_fields(mesh, rho, rhou, rhoe, "FvmEulerInletOutletBc")) return 1;
+    const int r = region_lookup(mesh, region);
+    if (r < 0) return 1;
+    enqueue_farfield(mesh, rho, rhou, rhoe, r, impl(rho)->cur, mach, pressure, temperature, t_stream);
+    return launch_ok("FvmEulerInletOutletBc") ? 0 : 1;
+}
+
+int FvmEulerStepPrepare(cuMesh* mesh, FvmField* rho, FvmField* rhou, FvmField* rhoe) {
+    clear_error();
+    if (!euler_fields(mesh, rho, rhou, rhoe, "FvmEulerStepPrepare")) return 1;
+    if (!ensure_grad(mesh, rho) || !ensure_grad(mesh, rhou) || !ensure_grad(mesh, rhoe)) return 1;
+    launch_grad_lim(impl(mesh)->dev, state_of(rho, rhou, rhoe, impl(rho)->cur), grad_of(rho, rhou, rhoe), t_stream);
+    return launch_ok("FvmEulerStepPrepare") ? 0 : 1;
+}
+
+int FvmEulerStep(cuMesh* mesh, FvmField* rho, FvmField* rhou, FvmField* rhoe, gb_scalar cfl, const char* time_scheme,
+                 FvmField* dt, FvmField* error) {
+    (void)dt;
+    clear_error();
+    if (!time_scheme || strcmp(time_scheme, "steady") != 0) {
+        set_error("FvmEulerStep: only the \"steady\" scheme exists");
+        return 1;
+    }
+    if (!euler_fields(mesh, rho, rhou, rhoe, "FvmEulerStep") || !bind(mesh, error, 1, "FvmEulerStep")) return 1;
+    if (!impl(rho)->grad || !impl(rhou)->grad || !impl(rhoe)->grad) {
+        set_error("FvmEulerStep: call FvmEulerStepPrepare first");
+        return 1;
+    }
+    FieldImpl* ei = impl(error);
+    const int nb = (int)((impl(mesh)->dev.N + kBlock - 1) / kBlock);
+    if (!ensure_partials(ei, std::max(nb, 1))) return 1;
+    const int cur = impl(rho)->cur;
+    enqueue_flux(mesh, rho, rhou, rhoe, error, cfl, cur, t_stream);
+    if (!launch_ok("FvmEulerStep")) return 1;
+    impl(rho)->cur = impl(rhou)->cur = impl(rhoe)->cur = 1 - cur;
+    ei->partials_valid = true;
+    return 0;
+}
+
+gb_scalar FvmFieldReduceSum(cuMesh* mesh, FvmField* var) {
+    clear_error();
+    const float nan = std::numeric_limits<float>::quiet_NaN();
+    if (!check_mesh(mesh) || !bind(mesh, var, 1, "FvmFieldReduceSum")) return nan;
+    FieldImpl* fi = impl(var);
+    MeshImpl* mi = impl(mesh);
+    cudaStream_t s = t_stream;
+    double* out = mi->dev.red + mi->dev.n_red_max;
+    if (fi->partials_valid) {
+        launch_reduce_final((int)((mi->dev.N + kBlock - 1) / kBlock), fi->partials, out, nullptr, nullptr, s);
+    } else {
+        const int nb = reduce_blocks(mi->dev.N);
+        launch_reduce_partials(mi->dev.N, (const float*)fi->val[fi->cur], mi->dev.red, s);
+        launch_reduce_final(nb, mi->dev.red, out, nullptr, nullptr, s);
+    }
+    double h = 0.0;
+    if (!launch_ok("FvmFieldReduceSum") ||
+        !cuda_ok(cudaMemcpyAsync(&h, out, sizeof(double), cudaMemcpyDeviceToHost, s), "FvmFieldReduceSum") ||
+        !cuda_ok(cudaStreamSynchronize(s), "FvmFieldReduceSum"))
+        return nan;
+    return (gb_scalar)h;
+}
+
+int64_t gbEulerRun(cuMesh* mesh, FvmField* rho, FvmField* rhou, FvmField* rhoe, FvmField* error, gb_scalar cfl,
+                   int64_t n_iter, const gbBc* bcs, int n_bc, double tolerance, int check_every,
+                   double* residual_history) {
+    clear_error();
+    if (n_iter < 0 || n_bc < 0 || (n_bc > 0 && !bcs)) { set_error("gbEulerRun: bad arguments"); return -1; }
+    if (!euler_fields(mesh, rho, rhou, rhoe, "gbEulerRun") || !bind(mesh, error, 1, "gbEulerRun")) return -1;
+    MeshImpl* mi = impl(mesh);
+    for (int b = 0; b < n_bc; ++b) {
+        if (bcs[b].region_id >= mi->topo.regions.size() || (bcs[b].type != 0 && bcs[b].type != 1)) {
+            set_error("gbEulerRun: bad boundary condition " + std::to_string(b));
+            return -1;
+        }
+    }
+    if (n_iter == 0) return 0;
+    if (!ensure_grad(mesh, rho) || !ensure_grad(mesh, rhou) || !ensure_grad(mesh, rhoe)) return -1;
+    FieldImpl* ei = impl(error);
+    const int nb = (int)((mi->dev.N + kBlock - 1) / kBlock);
+    if (!ensure_partials(ei, std::max(nb, 1))) return -1;
+    if (check_every <= 0) check_every = 100;
+    cudaStream_t s = t_stream;
+    double* d_hist = nullptr;
+    unsigned long long* d_counter = nullptr;
+    if (!dalloc(d_hist, (size_t)n_iter, "gbEulerRun") || !dalloc(d_counter, 1, "gbEulerRun") ||
+        !cuda_ok(cudaMemsetAsync(d_counter, 0, sizeof(unsigned long long), s), "gbEulerRun")) {
+        dfree(d_hist); dfree(d_counter);
+        return -1;
+    }
+    double* out = mi->dev.red + mi->dev.n_red_max;
+    // one graph per value buffer parity: BCs, gradients+limiters, flux+update, residual
+    cudaGraphExec_t exec[2] = {nullptr, nullptr};
+    cudaStream_t cap = nullptr;
+    bool ok = cuda_ok(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking), "gbEulerRun");
+    t_counting = false;
+    for (int k = 0; k < 2 && ok; ++k) {
+        cudaGraph_t g = nullptr;
+        ok = cuda_ok(cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal), "graph capture");
+        if (!ok) break;
+        for (int b = 0; b < n_bc; ++b) {
+            if (bcs[b].type == 0) enqueue_slip(mesh, rho, rhou, rhoe, (int)bcs[b].region_id, k, cap);
+            else enqueue_farfield(mesh, rho, rhou, rhoe, (int)bcs[b].region_id, k, bcs[b].mach, bcs[b].pressure,
+                                  bcs[b].temperature, cap);
+        }
+        launch_grad_lim(mi->dev, state_of(rho, rhou, rhoe, k), grad_of(rho, rhou, rhoe), cap);
+        enqueue_flux(mesh, rho, rhou, rhoe, error, cfl, k, cap);
+        launch_reduce_final(nb, ei->partials, out, d_hist, d_counter, cap);
+        ok = cuda_ok(cudaStreamEndCapture(cap, &g), "graph capture") &&
+             cuda_ok(cudaGraphInstantiate(&exec[k], g, 0), "graph instantiate");
+        if (g) cudaGraphDestroy(g);
+    }
+    t_counting = true;
+    const int per_iter = n_bc + 3;
+    int cur = impl(rho)->cur;
+    int64_t done = 0;
+    std::vector<double> hist((size_t)n_iter, 0.0);
+    while (ok && done < n_iter) {
+        const int64_t chunk = std::min<int64_t>(check_every, n_iter - done);
+        for (int64_t i = 0; i < chunk && ok; ++i) {
+            ok = cuda_ok(cudaGraphLaunch(exec[cur], s), "graph launch");
+            count_launch(per_iter);
+            cur = 1 - cur;
+        }
+        done += chunk;
+        if (!ok) break;
+        ok = cuda_ok(cudaMemcpyAsync(hist.data(), d_hist, done * sizeof(double), cudaMemcpyDeviceToHost, s), "gbEulerRun") &&
+             cuda_ok(cudaStreamSynchronize(s), "gbEulerRun");
+        if (ok && tolerance > 0.0 && hist[0] > 0.0) {
+            int64_t stop = -1;
+            for (int64_t i = done - chunk; i < done; ++i)
+                if (hist[i] / hist[0] < tolerance) { stop = i + 1; break; }
+            if (stop > 0) {
+                // iterations past `stop` in this chunk already ran; report all of them
+                break;
+            }
+        }
+        if (ok) {
+            bool bad = false;
+            for (int64_t i = done - chunk; i < done; ++i) bad |= !std::isfinite(hist[i]);
+            if (bad) { set_error("gbEulerRun: residual is not finite (diverged)"); ok = false; }
+        }
+    }
+    impl(rho)->cur = impl(rhou)->cur = impl(rhoe)->cur = cur;
+    ei->partials_valid = true;
+    if (residual_history) memcpy(residual_history, hist.data(), (size_t)done * sizeof(double));
+    for (int k = 0; k < 2; ++k) if (exec[k]) cudaGraphExecDestroy(exec[k]);
+    if (cap) cudaStreamDestroy(cap);
+    dfree(d_hist);
+    dfree(d_counter);
+    return ok ? done : -1;
+}
+
+}  // extern "C"

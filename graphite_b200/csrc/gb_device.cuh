@@ -1,0 +1,90 @@
+// Device data layout and kernel launchers of libgraphite_b200.so.
+//
+// Layout in HBM (all indices uint32, new = renumbered order):
+//   cell_geo  float4[N+G]   centroid xyz, volume            (interior, then ghosts)
+//   face_geo  float4[2F]    (unit normal xyz, area), (face centre xyz, 0)
+//   start     uint32[N+1]   interior cell -> first CSR entry
+//   nb        uint2[S]      (face, neighbour cell) per interior cell face, in
+//                           the reference's element-local face order
+//   lsq       float4[2N]    inverse LSQ matrix, symmetric: (a00 a01 a02 a11), (a12 a22 - -)
+//   ghost     uint2[G]      (interior cell, face) of each ghost
+// Fields (double-buffered values so that the update is a Jacobi sweep):
+//   scalar    float [N+G] x2
+//   vector    float4[N+G] x2 (xyz, pad)
+//   gradient  scalar: float4[N] (gradient xyz, limiter)
+//             vector: float4[3N], entry 3i+a = (gradient of component a, its limiter)
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+namespace gb {
+
+struct DevMesh {
+    int64_t N = 0, G = 0, F = 0, S = 0;
+    float4* cell_geo = nullptr;
+    float4* face_geo = nullptr;
+    uint32_t* start = nullptr;
+    uint2* nb = nullptr;
+    float4* lsq = nullptr;
+    uint2* ghost = nullptr;
+    // reduction scratch owned by the mesh
+    double* red = nullptr;        // n_red_max partials + 1 result
+    int n_red_max = 0;
+};
+
+// Pointers of the three conserved fields as one kernel argument.
+struct EulerState {
+    const float* rho;
+    const float4* rhou;
+    const float* rhoe;
+};
+
+struct EulerGrad {
+    float4* rho;     // N
+    float4* rhou;    // 3N
+    float4* rhoe;    // N
+};
+
+constexpr int kBlock = 256;
+
+int reduce_blocks(int64_t n);
+
+// ---- metrics (float64, reference order), metrics.cu ----
+void launch_face_metrics64(int64_t F, const double* nodes, const uint32_t* fns, const uint32_t* fn, double* area,
+                           double* normal, double* centre, cudaStream_t s);
+void launch_cell_metrics64(int64_t N, const uint32_t* cfs, const uint32_t* cf, const double* area,
+                           const double* normal, const double* fcentre, double* ccentre, double* volume,
+                           cudaStream_t s);
+void launch_ghost_metrics64(int64_t G, int64_t N, const uint32_t* cfs, const uint32_t* cf, const uint32_t* cc,
+                            const double* area, const double* normal, const double* fcentre, double* ccentre,
+                            double* volume, cudaStream_t s);
+void launch_lsq64(int64_t N, const uint32_t* cfs, const uint32_t* cc, const double* ccentre, double* minv,
+                  cudaStream_t s);
+void launch_layout(const DevMesh& m, const uint32_t* cell_old, const uint32_t* face_old, const double* area,
+                   const double* normal, const double* fcentre, const double* ccentre, const double* volume,
+                   const double* minv, cudaStream_t s);
+
+// ---- Euler path, euler.cu ----
+void launch_init(int64_t n, float* rho, float4* rhou, float* rhoe, float r, float3 ru, float e, cudaStream_t s);
+void launch_bc_slip(const DevMesh& m, uint32_t g0, uint32_t g1, float* rho[2], float4* rhou[2], float* rhoe[2],
+                    int cur, cudaStream_t s);
+void launch_bc_farfield(const DevMesh& m, uint32_t g0, uint32_t g1, float* rho[2], float4* rhou[2],
+                        float* rhoe[2], int cur, float3 mach, float p, float t, cudaStream_t s);
+void launch_grad_lim(const DevMesh& m, EulerState q, EulerGrad g, cudaStream_t s);
+void launch_flux(const DevMesh& m, EulerState q, EulerGrad g, float* rho_n, float4* rhou_n, float* rhoe_n,
+                 float* err, double* partials, float cfl, bool transposed, cudaStream_t s);
+void launch_reduce_partials(int64_t n, const float* v, double* partials, cudaStream_t s);
+void launch_reduce_final(int n_partials, const double* partials, double* out, double* history,
+                         unsigned long long* counter, cudaStream_t s);
+
+// permute helpers for host transfers (new <-> reference order)
+void launch_gather_scalar(int64_t n, const float* src, const uint32_t* idx, float* dst, cudaStream_t s);
+void launch_gather_vector(int64_t n, const float4* src, const uint32_t* idx, float* dst3, cudaStream_t s);
+void launch_scatter_scalar(int64_t n, const float* src, const uint32_t* idx, float* dst, cudaStream_t s);
+void launch_scatter_vector(int64_t n, const float* src3, const uint32_t* idx, float4* dst, cudaStream_t s);
+
+void count_launch(int n = 1);
+
+}  // namespace gb

@@ -1,0 +1,169 @@
+"""The reference's PhysicsEuler driver loop, over the C ABI.
+
+``EulerCase`` does what PhysicsEuler (src/models/euler.cu:12-175) does with
+the reference's entry points -- load the mesh, create rho/rhou/rhoe/error,
+initialise from a free stream, and per iteration apply the boundary
+conditions, prepare gradients and limiters, step, and reduce the residual --
+but calls libgraphite_b200.so.  ``run`` uses the graph-replayed loop
+(gbEulerRun) instead of one C call per stage.
+
+Boundary conditions are tuples ``("slip", region)`` or
+``("farfield", region, mach_x, mach_y, mach_z, pressure, temperature)``.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import tempfile
+from typing import Sequence, Tuple
+
+import numpy as np
+
+from . import capi
+
+
+class EulerCase:
+    def __init__(self, mesh_path: str, via_fvm: bool = True):
+        """Load an SU2 mesh, either through cuMeshFromSu2 + cuMeshFromFile
+        (the reference's path, float32 node coordinates) or directly."""
+        lib = capi.load()
+        self.lib = lib
+        self._tmp = None
+        if mesh_path.endswith(".su2") and via_fvm:
+            self._tmp = tempfile.mkdtemp(prefix="gb_mesh_")
+            fvm = os.path.join(self._tmp, os.path.basename(mesh_path)[:-3] + "fvm")
+            capi.check(lib.cuMeshFromSu2(mesh_path.encode(), fvm.encode()), "cuMeshFromSu2")
+            mesh = lib.cuMeshFromFile(fvm.encode())
+        elif mesh_path.endswith(".su2"):
+            mesh = lib.gbMeshFromSu2(mesh_path.encode())
+        else:
+            mesh = lib.cuMeshFromFile(mesh_path.encode())
+        if not mesh:
+            raise capi.GraphiteError(f"mesh load failed: {capi.last_error()}")
+        self.mesh = mesh
+        base = mesh.contents._cpu.contents
+        self.n_cells = int(base.n_cells)
+        self.n_ghosts = int(base.n_ghosts)
+        self.n_faces = int(base.n_faces)
+        n = int(lib.cuMeshGetVarSize(mesh))
+        self.rho = lib.FvmFieldNew(4, n, b"rho", 1)
+        self.rhou = lib.FvmFieldNew(12, n, b"rhou", 1)
+        self.rhoe = lib.FvmFieldNew(4, n, b"rhoe", 1)
+        self.error = lib.FvmFieldNew(4, n, b"error", 1)
+        if not (self.rho and self.rhou and self.rhoe and self.error):
+            raise capi.GraphiteError(f"FvmFieldNew failed: {capi.last_error()}")
+        self.err0 = None
+
+    @property
+    def regions(self):
+        m = self.mesh.contents
+        return [m.region_names[i].decode() for i in range(m.region_names_size)]
+
+    def init(self, mach: Sequence[float], pressure: float, temperature: float) -> None:
+        capi.check(self.lib.FvmEulerInit(self.mesh, self.rho, self.rhou, self.rhoe, capi.vec(mach), pressure,
+                                         temperature), "FvmEulerInit")
+
+    def set_state(self, rho: np.ndarray, rhou: np.ndarray, rhoe: np.ndarray) -> None:
+        """Upload a state given in reference order (cells then ghosts)."""
+        for f, v in ((self.rho, rho), (self.rhou, rhou), (self.rhoe, rhoe)):
+            capi.set_field_values(f, v)
+            capi.check(self.lib.gbVarCpuToGpu(self.mesh, f), "gbVarCpuToGpu")
+
+    def apply_bcs(self, bcs) -> None:
+        for b in bcs:
+            if b[0] == "slip":
+                rc = self.lib.FvmEulerSlipBc(self.mesh, self.rho, self.rhou, self.rhoe, b[1].encode())
+            else:
+                rc = self.lib.FvmEulerInletOutletBc(self.mesh, self.rho, self.rhou, self.rhoe, capi.vec(b[2:5]),
+                                                    float(b[5]), float(b[6]), b[1].encode())
+            capi.check(rc, f"boundary condition {b[0]} on {b[1]}")
+
+    def prepare(self) -> None:
+        capi.check(self.lib.FvmEulerStepPrepare(self.mesh, self.rho, self.rhou, self.rhoe), "FvmEulerStepPrepare")
+
+    def step(self, cfl: float) -> None:
+        capi.check(self.lib.FvmEulerStep(self.mesh, self.rho, self.rhou, self.rhoe, cfl, b"steady", None,
+                                         self.error), "FvmEulerStep")
+
+    def residual(self) -> float:
+        r = float(self.lib.FvmFieldReduceSum(self.mesh, self.error))
+        if r != r:
+            raise capi.GraphiteError(f"FvmFieldReduceSum failed: {capi.last_error()}")
+        return r
+
+    def iterate(self, bcs, cfl: float) -> float:
+        """One PhysicsEuler::step (src/models/euler.cu:99-175); returns the
+        residual sum of this iteration."""
+        self.apply_bcs(bcs)
+        self.prepare()
+        self.step(cfl)
+        return self.residual()
+
+    def bc_structs(self, bcs):
+        arr = (capi.gbBc * max(len(bcs), 1))()
+        for i, b in enumerate(bcs):
+            rid = self.lib.cuMeshGetRegionId(self.mesh, b[1].encode())
+            if rid == 0xFFFFFFFF:
+                raise capi.GraphiteError(capi.last_error())
+            if b[0] == "slip":
+                arr[i] = capi.gbBc(0, rid, capi.vec(0, 0, 0), 0.0, 0.0)
+            else:
+                arr[i] = capi.gbBc(1, rid, capi.vec(b[2:5]), float(b[5]), float(b[6]))
+        return arr
+
+    def run(self, bcs, cfl: float, n_iter: int, tolerance: float = 0.0, check_every: int = 100) -> np.ndarray:
+        """n_iter iterations as replayed CUDA graphs; returns the residual
+        history (stops early below ``tolerance`` relative to the first)."""
+        arr = self.bc_structs(bcs)
+        hist = np.zeros(max(n_iter, 1), dtype=np.float64)
+        done = self.lib.gbEulerRun(self.mesh, self.rho, self.rhou, self.rhoe, self.error, cfl, n_iter, arr, len(bcs),
+                                   tolerance, check_every, hist.ctypes.data_as(C.POINTER(C.c_double)))
+        if done < 0:
+            raise capi.GraphiteError(f"gbEulerRun failed: {capi.last_error()}")
+        return hist[:done]
+
+    def fields(self) -> Tuple[np.ndarray, np.ndarray, np.ndarray]:
+        """(rho, rhou, rhoe) in reference order, cells then ghosts."""
+        out = []
+        for f in (self.rho, self.rhou, self.rhoe):
+            self.lib.VarGpuToCpu(f)
+            if capi.last_error():
+                raise capi.GraphiteError(capi.last_error())
+            out.append(capi.field_values(f))
+        return tuple(out)
+
+    def gradients(self):
+        """{name: (gradient, limiter)} after VarAllGpuToCpu, reference layout."""
+        out = {}
+        for name, f in (("rho", self.rho), ("rhou", self.rhou), ("rhoe", self.rhoe)):
+            self.lib.VarAllGpuToCpu(f)
+            out[name] = capi.field_gradients(f)
+        return out
+
+    def error_values(self) -> np.ndarray:
+        self.lib.VarGpuToCpu(self.error)
+        return capi.field_values(self.error)
+
+    def close(self) -> None:
+        if getattr(self, "mesh", None):
+            for f in (self.rho, self.rhou, self.rhoe, self.error):
+                if f:
+                    self.lib.FvmFieldFree(f)
+            self.lib.cuMeshFree(self.mesh)
+            self.mesh = None
+        if self._tmp:
+            import shutil
+            shutil.rmtree(self._tmp, ignore_errors=True)
+            self._tmp = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

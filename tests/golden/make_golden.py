@@ -9,7 +9,8 @@ in a tree where the reference sources are present; the built
 For each case in cases.py it writes the SU2 mesh, runs the driver in one of
 its modes and stores the arrays as ``<case>_<mode>.npz``:
 
-* metrics  - the reference's mesh arrays after cuMeshFromSu2/cuMeshFromFile
+* metrics  - the reference converter's .fvm file (``<case>_ref.fvm``) and
+             the reference's mesh arrays after cuMeshFromSu2/cuMeshFromFile
              (CSR topology, face areas/normals/centres, cell volumes/centres,
              inverse LSQ matrices), for every element kind;
 * prepare  - value/gradient/limiter of rho, rhou, rhoe after the boundary
@@ -21,6 +22,7 @@ from __future__ import annotations
 
 import argparse
 import os
+import shutil
 import subprocess
 import sys
 import time
@@ -87,6 +89,8 @@ def main():
             out = os.path.join(a.work, f"{name}_metrics.bin")
             run([DRIVER, case, path, out, "metrics"], log)
             rec = refio.read_records(out)
+            # the reference converter's own .fvm output, for the converter tests
+            shutil.copyfile(path[:-3] + "fvm", os.path.join(a.out, f"{name}_ref.fvm"))
             np.savez_compressed(os.path.join(a.out, f"{name}_metrics.npz"), sizes=rec["sizes"],
                                 **{k: rec[k] for k in FLOAT_KEYS_METRICS + INT_KEYS_METRICS})
     if "prepare" in only:

@@ -1,0 +1,119 @@
+"""The C ABI without a GPU: exported symbols, the SU2 -> .fvm converter
+against the reference converter's own output, and error reporting."""
+import os
+
+import numpy as np
+import pytest
+
+import cases
+from graphite_b200 import capi
+from helpers import read_fvm
+
+GOLDEN = os.path.dirname(cases.__file__)
+
+
+def test_library_exports_every_declared_function():
+    lib = capi.load()
+    names = capi.header_functions()
+    assert len(names) >= 30
+    missing = [n for n in names if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+def test_struct_layout_matches_header():
+    # cuMeshBase: 2 ints, 5 size_t, 14 pointers; FvmField: 4 pointers + impl
+    import ctypes as C
+    assert C.sizeof(capi.gb_vector) == 12
+    assert C.sizeof(capi.gb_tensor) == 36
+    assert C.sizeof(capi.cuMeshBase) == 8 + 5 * 8 + 14 * 8
+    assert C.sizeof(capi.FvmField) == 5 * 8
+    assert C.sizeof(capi.gbBc) == 4 + 4 + 12 + 4 + 4
+
+
+@pytest.mark.parametrize("name", ["tet_6x3x2", "hex_6x3x2", "prism_6x3x2", "pyramid_6x3x2", "tet_12x6x2"])
+def test_converter_matches_reference_converter(name, su2_paths, workdir):
+    """cuMeshFromSu2 writes the file the reference's converter writes: same
+    float32 nodes, same faces with the same node order, same cells (face
+    lists in element-local order, neighbours), same regions; faces are
+    numbered in first-appearance order instead of hash-bucket order."""
+    out = str(workdir / f"{name}_mine.fvm")
+    assert capi.load().cuMeshFromSu2(su2_paths(name).encode(), out.encode()) == 0, capi.last_error()
+    rn, rf, rc, rr = read_fvm(os.path.join(GOLDEN, f"{name}_ref.fvm"))
+    mn, mf, mc, mr = read_fvm(out)
+    assert np.array_equal(rn, mn)
+    key = {tuple(sorted(f)): i for i, f in enumerate(rf)}
+    perm = [key[tuple(sorted(f))] for f in mf]          # my face -> reference face
+    assert sorted(perm) == list(range(len(rf)))
+    for i, f in enumerate(mf):
+        assert rf[perm[i]] == f
+    assert len(rc) == len(mc)
+    for (rfaces, rconn), (mfaces, mconn) in zip(rc, mc):
+        assert tuple(perm[f] for f in mfaces) == rfaces
+        assert mconn == rconn
+    assert rr == mr
+
+
+def _write(path, text):
+    with open(path, "w") as f:
+        f.write(text)
+    return path
+
+
+def test_converter_errors(workdir):
+    lib = capi.load()
+    out = str(workdir / "bad.fvm").encode()
+    assert lib.cuMeshFromSu2(b"/nonexistent/mesh.su2", out) != 0
+    assert "cannot open" in capi.last_error()
+    p = _write(str(workdir / "dim2.su2"), "NDIME= 2\n")
+    assert lib.cuMeshFromSu2(p.encode(), out) != 0 and "3D" in capi.last_error()
+    # a single tet with no boundary markers: open mesh
+    tet = "NDIME= 3\nNELEM= 1\n10 0 1 2 3 0\nNPOIN= 4\n0 0 0 0\n1 0 0 1\n0 1 0 2\n0 0 1 3\n"
+    p = _write(str(workdir / "open.su2"), tet)
+    assert lib.cuMeshFromSu2(p.encode(), out) != 0 and "open mesh" in capi.last_error()
+    # node index out of range
+    p = _write(str(workdir / "range.su2"), tet.replace("10 0 1 2 3 0", "10 0 1 2 9 0"))
+    assert lib.cuMeshFromSu2(p.encode(), out) != 0 and "out of range" in capi.last_error()
+    # unknown element kind
+    p = _write(str(workdir / "kind.su2"), tet.replace("10 0 1 2 3 0", "11 0 1 2 3 0"))
+    assert lib.cuMeshFromSu2(p.encode(), out) != 0 and "kind" in capi.last_error()
+    # a marker face that matches no element face
+    closed = tet + "NMARK= 1\nMARKER_TAG= wall\nMARKER_ELEMS= 1\n9 0 1 2 3\n"
+    p = _write(str(workdir / "nomatch.su2"), closed)
+    assert lib.cuMeshFromSu2(p.encode(), out) != 0 and "matches no element face" in capi.last_error()
+    # the same boundary face listed twice
+    twice = tet + "NMARK= 1\nMARKER_TAG= wall\nMARKER_ELEMS= 2\n5 0 2 1\n5 1 0 2\n"
+    p = _write(str(workdir / "twice.su2"), twice)
+    assert lib.cuMeshFromSu2(p.encode(), out) != 0 and "already has two cells" in capi.last_error()
+    # the closed single tet converts
+    ok = tet + "NMARK= 1\nMARKER_TAG= wall\nMARKER_ELEMS= 4\n5 0 2 1\n5 0 1 3\n5 1 2 3\n5 0 3 2\n"
+    p = _write(str(workdir / "ok.su2"), ok)
+    assert lib.cuMeshFromSu2(p.encode(), out) == 0, capi.last_error()
+    nodes, faces, cells, regions = read_fvm(out.decode())
+    assert len(faces) == 4 and len(cells) == 5 and regions[0][0] == "wall"
+    assert cells[0][1] == (1, 2, 3, 4)       # each face of the tet leads to its ghost
+
+
+def test_fvm_reader_rejects_corrupt_files(workdir):
+    lib = capi.load()
+    p = str(workdir / "trunc.fvm")
+    data = open(os.path.join(GOLDEN, "tet_6x3x2_ref.fvm"), "rb").read()
+    with open(p, "wb") as f:
+        f.write(data[: len(data) // 2])
+    assert not lib.cuMeshFromFile(p.encode())
+    assert "truncated" in capi.last_error() or "bad" in capi.last_error()
+    assert not lib.cuMeshFromFile(b"/nonexistent/x.fvm")
+    assert "cannot open" in capi.last_error()
+
+
+def test_field_api_without_gpu_reports_errors():
+    """FvmFieldNew needs device memory; without a GPU it fails loudly (NULL
+    with a CUDA message), never silently."""
+    import torch
+
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    lib = capi.load()
+    assert not lib.FvmFieldNew(4, 10, b"rho", 1)
+    assert capi.last_error()
+    assert not lib.FvmFieldNew(7, 10, b"bad", 1)
+    assert "elem_size" in capi.last_error()
