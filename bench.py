@@ -1,0 +1,454 @@
+"""Benchmark: cell-updates/s of the explicit second-order Euler iteration.
+
+Workload (default): the transonic swept wing -- NACA 0012, chord 1, semispan
+1.5, 30 deg leading-edge sweep, taper 0.56, Mach 0.84, AoA 3 deg, CFL 0.8 --
+on the procedural 1,116,032-cell mesh of graphite_b200.meshgen.swept_wing
+(synthetic: the reference's wing mesh is built from a CAD file with gmsh,
+which is not available).  One step = one full iteration (boundary
+conditions, gradients + limiters, flux + local-time-step update, residual
+sum) over every cell of the mesh.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+ours: `value` is device-timed (CUDA events on the library's stream) over K
+graph-replayed iterations with the state resident in HBM; `e2e` runs the
+reference's per-call loop through the C ABI (one C call per stage and a
+residual read back to the host every iteration, as apps/main.cu does) with
+the initial state uploaded from pinned host memory and the final state read
+back inside the timed region.  `roofline` times the dominant kernel with CUDA
+events; `cpu_baseline` times the oracle (a C++ restatement of the reference's
+kernels; the reference itself has no CPU path) on the host cores on a bounded
+sample.  Multi-GPU: replicas (one mesh per GPU, no exchange), weak scaling.
+
+reference: the same metric from the oracle port on the host cores (rank 0
+only), each step one bounded sample (a contiguous block of cells) of the
+iteration.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+MACH, AOA_DEG, CFL = 0.84, 3.0, 0.8
+P_INF, T_INF = 1.0, 1.0 / 1.4
+WORKLOADS = {
+    "swept_wing": dict(desc="swept NACA 0012 wing, 1,116,032 prisms, M 0.84, AoA 3 deg, CFL 0.8"),
+    "channel": dict(desc="channel with 10% bump, 28,800 tets, M 0.5, CFL 0.8"),
+    "airfoil_120k": dict(desc="NACA 0012 airfoil, 120,000 prisms (one layer), M 0.84, AoA 3 deg, CFL 0.8"),
+}
+HBM_FALLBACK_GBS = 6650.0
+
+
+def freestream():
+    a = math.radians(AOA_DEG)
+    return (MACH * math.cos(a), 0.0, MACH * math.sin(a))
+
+
+BC_NAMES = {
+    "swept_wing": [("farfield", "farfield"), ("slip", "symmetry"), ("slip", "wing")],
+    "channel": [("farfield", "inlet"), ("slip", "lower"), ("farfield", "outlet"), ("slip", "sides"),
+                ("slip", "upper")],
+    "airfoil_120k": [("farfield", "farfield"), ("slip", "sides"), ("slip", "wing")],
+}
+
+
+def case_bcs(name):
+    """(boundary conditions in the reference's sorted-key order, free-stream Mach)."""
+    mach = (0.5, 0.0, 0.0) if name == "channel" else freestream()
+    bcs = [(t, r) + (tuple(mach) + (P_INF, T_INF) if t == "farfield" else ()) for t, r in BC_NAMES[name]]
+    return bcs, mach
+
+
+def build_mesh(name):
+    from graphite_b200 import meshgen
+    if name == "swept_wing":
+        m = meshgen.swept_wing()
+    elif name == "channel":
+        m = meshgen.channel_bump()
+    elif name == "airfoil_120k":
+        m = meshgen.airfoil_extruded(120_000)
+    else:
+        raise SystemExit(f"unknown workload {name}")
+    bcs, mach = case_bcs(name)
+    return m, bcs, mach
+
+
+def mesh_file(name, cache):
+    """SU2 file of the workload's mesh, generated once per machine."""
+    path = os.path.join(cache, f"{name}.su2")
+    if not os.path.exists(path):
+        m, _, _ = build_mesh(name)
+        tmp = path + f".tmp{os.getpid()}"
+        m.write_su2(tmp)
+        os.replace(tmp, path)
+    bcs, mach = case_bcs(name)
+    return path, bcs, mach
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return HBM_FALLBACK_GBS, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi samples of SM clock and throttle reasons during a region."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "50"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+            time.sleep(0.3)
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            time.sleep(0.15)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 7:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                mx.append(float(parts[1]))
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[3:7]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def byte_model(case):
+    """Algorithmic bytes per launch of the two hot kernels (each array element
+    of the device layout touched once)."""
+    N, G, F = case.n_cells, case.n_ghosts, case.n_faces
+    S = int(case.mesh.contents._cpu.contents.cell_faces_starts[N])  # interior cell-face entries
+    NG = N + G
+    state = 4 + 16 + 4          # rho, rhou (float4), rhoe
+    grad_lim = {
+        "cell_geo": 16 * NG, "state": state * NG, "csr": 4 * (N + 1) + 8 * S, "lsq": 32 * N,
+        "face_centre": 16 * F, "grad_write": 80 * N}
+    flux = {
+        "cell_geo": 16 * NG, "state": state * NG, "grad": 80 * N, "csr": 4 * (N + 1) + 8 * S,
+        "face_geo": 32 * F, "state_write": state * N, "err_write": 4 * N, "partials": 8 * ((N + 255) // 256)}
+    return {"k_grad_lim": sum(grad_lim.values()), "k_flux": sum(flux.values()),
+            "detail": {"k_grad_lim": grad_lim, "k_flux": flux}, "S": S}
+
+
+def ncu_traffic(kernel, workload):
+    """DRAM bytes per launch from a committed ncu summary (profiles/), if any:
+    a line `traffic_bytes_per_launch <kernel> <workload> <bytes>`."""
+    path = os.path.join(ROOT, "profiles", "ncu_traffic.txt")
+    try:
+        for ln in open(path):
+            p = ln.split()
+            if len(p) == 4 and p[0] == "traffic_bytes_per_launch" and p[1] == kernel and p[2] == workload:
+                return float(p[3])
+    except OSError:
+        pass
+    return None
+
+
+def run_ours(args, rank, world, local_rank):
+    import torch
+
+    torch.cuda.set_device(local_rank)
+    from graphite_b200 import capi
+    from graphite_b200.euler import EulerCase
+
+    lib = capi.load()
+    dev_stream = torch.cuda.current_stream()
+    lib.gbSetStream(C_void(dev_stream.cuda_stream))
+    cache = os.path.join(tempfile.gettempdir(), "graphite_b200_bench")
+    os.makedirs(cache, exist_ok=True)
+    if rank == 0:
+        mesh_file(args.workload, cache)
+    if world > 1:
+        torch.distributed.barrier()
+    path, bcs, mach = mesh_file(args.workload, cache)
+    t0 = time.perf_counter()
+    case = EulerCase(path, via_fvm=True)
+    setup_s = time.perf_counter() - t0
+    N = case.n_cells
+    K, W = args.steps, args.warmup
+
+    # ---- value: K graph-replayed iterations, state resident in HBM ----
+    case.init(mach, P_INF, T_INF)
+    case.run(bcs, CFL, W, check_every=max(W, 1))
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    launches0 = lib.gbKernelLaunchCount()
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local_rank) as clocks:
+        ev0.record(dev_stream)
+        hist = case.run(bcs, CFL, K, check_every=K)
+        ev1.record(dev_stream)
+        torch.cuda.synchronize()
+    launches = lib.gbKernelLaunchCount() - launches0
+    t_ms = ev0.elapsed_time(ev1)
+    if world > 1:
+        t = torch.tensor([t_ms], device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        t_ms = float(t.item())
+        torch.distributed.barrier()
+    finite = bool(np.all(np.isfinite(hist)))
+
+    # ---- roofline: per-kernel device time of the per-call stages ----
+    bm = byte_model(case)
+    n_k = min(max(K // 4, 20), 400)
+    pe = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+    t_prep, t_flux = 0.0, 0.0
+    for _ in range(n_k):
+        case.apply_bcs(bcs)
+        pe[0].record(dev_stream)
+        case.prepare()
+        pe[1].record(dev_stream)
+        case.step(CFL)
+        pe[2].record(dev_stream)
+        pe[2].synchronize()
+        t_prep += pe[0].elapsed_time(pe[1])
+        t_flux += pe[1].elapsed_time(pe[2])
+    t_prep /= n_k
+    t_flux /= n_k
+    peak, peak_kind = measured_peaks()
+    dominant = "k_flux" if t_flux >= t_prep else "k_grad_lim"
+    t_dom = t_flux if dominant == "k_flux" else t_prep
+    achieved = bm[dominant] / (t_dom * 1e-3) / 1e9
+    traffic = ncu_traffic(dominant, args.workload)
+
+    # ---- e2e: the apps/main.cu loop through the C ABI from host buffers ----
+    case.init(mach, P_INF, T_INF)
+    rho0, rhou0, rhoe0 = case.fields()     # initial state in pinned host mirrors
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    te0 = time.perf_counter()
+    case.set_state(rho0, rhou0, rhoe0)     # H2D from the pinned mirrors
+    for _ in range(K):
+        case.iterate(bcs, CFL)             # BCs, prepare, step, residual -> host
+    rho1, rhou1, rhoe1 = case.fields()     # D2H of the final state
+    te = time.perf_counter() - te0
+    if world > 1:
+        t = torch.tensor([te], device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        te = float(t.item())
+    state_bytes = (rho0.nbytes + rhou0.nbytes + rhoe0.nbytes)
+    e2e = {"value": world * N * K / te, "unit": "cell-updates/s",
+           "h2d_bytes_per_step": state_bytes / K, "d2h_bytes_per_step": 8 + state_bytes / K,
+           "path": "per-call C ABI (FvmEuler*Bc, FvmEulerStepPrepare, FvmEulerStep, FvmFieldReduceSum) "
+                   "with the state uploaded from and read back to pinned host memory"}
+
+    # ---- time to a 1e-3 residual drop (reference's squared residual) ----
+    ttr = None
+    if rank == 0 and not args.skip_convergence:
+        case.init(mach, P_INF, T_INF)
+        c0, c1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        c0.record(dev_stream)
+        h = case.run(bcs, CFL, args.max_iters, tolerance=1e-3, check_every=100)
+        c1.record(dev_stream)
+        torch.cuda.synchronize()
+        ratio = h / h[0]
+        reached = bool(np.any(ratio < 1e-3))
+        it = int(np.argmax(ratio < 1e-3)) + 1 if reached else len(h)
+        ttr = {"reached": reached, "iterations": it, "seconds": c0.elapsed_time(c1) * 1e-3 * it / len(h),
+               "min_residual_ratio": float(np.min(ratio)), "max_iterations": args.max_iters,
+               "metric": "sum over cells of (F_rho^2+|F_rhou|^2+F_rhoE^2) V, relative to iteration 0"}
+
+    # ---- CPU baseline (rank 0, N = 1) ----
+    cpu = None
+    if rank == 0 and world == 1 and not args.skip_cpu:
+        cpu = cpu_baseline(args.workload, max_seconds=args.cpu_seconds)
+
+    value = world * N * K / (t_ms * 1e-3)
+    out = {
+        "metric": "cell-updates/s", "value": value, "unit": "cell-updates/s", "n_gpus": world, "steps": K,
+        "warmup": W, "ms_per_step": t_ms / K, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32 (f64 metrics and reductions)",
+        "data": "synthetic procedural mesh and uniform free-stream start",
+        "config": {"workload": args.workload, "description": WORKLOADS[args.workload]["desc"], "cells": N,
+                   "ghosts": case.n_ghosts, "faces": case.n_faces, "cfl": CFL, "parallelism": f"replicas x{world}",
+                   "l2": "inputs larger than L2: %.0f MB resident on the device" % resident_mb(case, bm),
+                   "mesh_setup_seconds": setup_s},
+        "e2e": e2e,
+        "gpu_launches": int(launches),
+        "roofline": {"bound": "hbm", "kernel": dominant, "achieved": achieved, "peak": peak,
+                     "peak_source": peak_kind, "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
+                     "algorithmic_bytes_per_launch": bm[dominant], "ms_per_launch": t_dom,
+                     "other_kernel": {"name": "k_grad_lim" if dominant == "k_flux" else "k_flux",
+                                      "ms_per_launch": t_prep if dominant == "k_flux" else t_flux,
+                                      "algorithmic_bytes_per_launch": bm["k_grad_lim" if dominant == "k_flux" else "k_flux"]}},
+        "clocks": clocks.summary(),
+        "residual_finite": finite,
+        "time_to_1e-3": ttr,
+        "cpu_baseline": cpu,
+    }
+    case.close()
+    return out
+
+
+def resident_mb(case, bm):
+    N, G, F = case.n_cells, case.n_ghosts, case.n_faces
+    S = bm["S"]
+    return (2 * 24 * (N + G) + 80 * N + 16 * (N + G) + 32 * F + 4 * N + 8 * S + 32 * N + 8 * G + 4 * (N + G)) / 1e6
+
+
+def C_void(x):
+    import ctypes
+    return ctypes.c_void_p(int(x))
+
+
+def cpu_baseline(workload, max_seconds=20.0, sample_cells=None):
+    """The oracle (float32, OpenMP on all host threads) on bounded samples of
+    one iteration: returns the cell-updates/s it sustains."""
+    import oracle.pyoracle as po
+    from oracle import OracleMesh, OracleSolver
+
+    m, bcs, mach = build_mesh(workload)
+    om = OracleMesh(m, metric_bits=64)
+    s = OracleSolver(om, bits=32)
+    s.init(mach, P_INF, T_INF)
+    s.apply_bcs(bcs)
+    N = om.N
+    block = sample_cells or min(N, 65536)
+    s.sample_step(CFL, 0, block)          # warm-up
+    done, t0, c = 0, time.perf_counter(), 0
+    while time.perf_counter() - t0 < max_seconds:
+        c1 = min(N, c + block)
+        s.sample_step(CFL, c, c1)
+        done += c1 - c
+        c = 0 if c1 >= N else c1
+    dt = time.perf_counter() - t0
+    return {"value": done / dt, "unit": "cell-updates/s", "cores": po.max_threads(), "kind": "port",
+            "sample": f"{done} cell-updates in blocks of {block} cells of the {N}-cell mesh over {dt:.1f} s "
+                      "(gradients, limiters, flux and update; float32)"}
+
+
+def run_reference(args, rank, world):
+    """The oracle port on the host cores: each step is one bounded sample (a
+    block of cells) of the iteration."""
+    if rank != 0:
+        return None
+    import oracle.pyoracle as po
+    from oracle import OracleMesh, OracleSolver
+
+    m, bcs, mach = build_mesh(args.workload)
+    om = OracleMesh(m, metric_bits=64)
+    s = OracleSolver(om, bits=32)
+    s.init(mach, P_INF, T_INF)
+    s.apply_bcs(bcs)
+    N = om.N
+    block = min(N, 8192)
+    c = 0
+    for _ in range(args.warmup):
+        s.sample_step(CFL, c, min(N, c + block))
+        c = (c + block) % N
+    t0 = time.perf_counter()
+    done = 0
+    for _ in range(args.steps):
+        c1 = min(N, c + block)
+        s.sample_step(CFL, c, c1)
+        done += c1 - c
+        c = 0 if c1 >= N else c1
+    dt = time.perf_counter() - t0
+    v = done / dt
+    return {"metric": "cell-updates/s", "value": v, "unit": "cell-updates/s", "impl": "reference",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3 / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic procedural mesh and uniform free-stream start",
+            "config": {"workload": args.workload, "description": WORKLOADS[args.workload]["desc"], "cells": N,
+                       "parallelism": "host cores", "sample_block_cells": block},
+            "cpu_baseline": {"value": v, "unit": "cell-updates/s", "cores": po.max_threads(), "kind": "port",
+                             "sample": f"{args.steps} blocks of {block} cells (one block per step)"},
+            "e2e": {"value": v, "unit": "cell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "note": "the reference has no host implementation of this path (all of it is CUDA); this is the "
+                    "oracle, a C++ restatement of the reference's kernels, with OpenMP over cells"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3000)
+    ap.add_argument("--warmup", type=int, default=50)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="swept_wing", choices=list(WORKLOADS))
+    ap.add_argument("--max-iters", type=int, default=10000, help="cap for the time-to-1e-3 run")
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--skip-cpu", action="store_true")
+    ap.add_argument("--skip-convergence", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        out = run_reference(args, rank, world)
+        if rank == 0:
+            print(json.dumps(out), flush=True)
+        return
+    if world > 1:
+        import datetime
+        import torch
+        torch.cuda.set_device(local_rank)
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    out = run_ours(args, rank, world, local_rank)
+    if world > 1:
+        import torch
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+
+
+if __name__ == "__main__":
+    main()

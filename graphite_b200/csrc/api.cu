@@ -489,13 +489,15 @@ FvmField* FvmFieldNew(size_t elem_size, size_t size, const char* name, int alloc
     f->_cpu = hmalloc<FvmFieldBase>(1);
     f->_cpu->elem_size = elem_size;
     f->_cpu->size = size;
-    f->_cpu->value = calloc(size ? size : 1, elem_size);
+    // the value mirror is pinned so that VarGpuToCpu / gbVarCpuToGpu run at
+    // full PCIe/C2C bandwidth
+    bool ok = cuda_ok(cudaMallocHost(&f->_cpu->value, (size ? size : 1) * elem_size), "FvmFieldNew");
+    if (ok) memset(f->_cpu->value, 0, (size ? size : 1) * elem_size);
     if (alloc_grads) {
         f->_cpu->gradient = calloc(size ? size : 1, elem_size * 3);
         f->_cpu->limiter = calloc(size ? size : 1, elem_size);
     }
     const size_t vb = comps == 1 ? sizeof(float) : sizeof(float4);
-    bool ok = true;
     for (int k = 0; k < 2 && ok; ++k) {
         ok = cuda_ok(cudaMalloc(&fi->val[k], (size ? size : 1) * vb), "FvmFieldNew") &&
              cuda_ok(cudaMemsetAsync(fi->val[k], 0, (size ? size : 1) * vb, t_stream), "FvmFieldNew");
@@ -515,7 +517,8 @@ void FvmFieldFree(FvmField* f) {
         delete fi;
     }
     if (f->_cpu) {
-        free(f->_cpu->value); free(f->_cpu->gradient); free(f->_cpu->limiter);
+        if (f->_cpu->value) cudaFreeHost(f->_cpu->value);
+        free(f->_cpu->gradient); free(f->_cpu->limiter);
         free(f->_cpu);
     }
     free(f->name);

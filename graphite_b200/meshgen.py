@@ -288,14 +288,15 @@ def channel_bump(nx: int = 60, ny: int = 20, nz: int = 4, length: float = 3.0, h
 # ---------------------------------------------------------------------------
 # NACA 0012 sections.
 # ---------------------------------------------------------------------------
-def naca0012_contour(n: int, closed_te: bool = True) -> Tuple[np.ndarray, np.ndarray]:
+def naca0012_contour(n: int, closed_te: bool = True, cluster: float = 1.0) -> Tuple[np.ndarray, np.ndarray]:
     """O-grid contour with ``n`` points (n even), index 0 at the trailing edge,
     running over the upper surface to the leading edge (n/2) and back along
-    the lower surface.  Cosine clustering at both edges; unit chord."""
+    the lower surface; unit chord.  Points are a blend of cosine clustering at
+    both edges (weight ``cluster``) and even spacing in x."""
     assert n % 2 == 0
     half = n // 2
     beta = np.linspace(0.0, math.pi, half + 1)
-    x = 0.5 * (1.0 + np.cos(beta))          # 1 -> 0 (TE to LE)
+    x = cluster * 0.5 * (1.0 + np.cos(beta)) + (1.0 - cluster) * (1.0 - beta / math.pi)   # TE -> LE
     a4 = -0.1036 if closed_te else -0.1015
     t = 0.6 * (0.2969 * np.sqrt(x) - 0.1260 * x - 0.3516 * x ** 2 + 0.2843 * x ** 3 + a4 * x ** 4)
     xu, zu = x, t
@@ -320,6 +321,44 @@ def _radial(n: int, first: float, total: float) -> np.ndarray:
     return d * (total / d[-1])
 
 
+
+def _contour_normals(xc: np.ndarray, zc: np.ndarray) -> Tuple[np.ndarray, np.ndarray]:
+    """Outward unit normals of a closed contour (either orientation),
+    averaged over the two edges at each point."""
+    px, pz = np.roll(xc, 1), np.roll(zc, 1)
+    nx_, nz_ = np.roll(xc, -1), np.roll(zc, -1)
+    e1 = np.stack([xc - px, zc - pz], 1)
+    e2 = np.stack([nx_ - xc, nz_ - zc], 1)
+    e1 /= np.linalg.norm(e1, axis=1, keepdims=True)
+    e2 /= np.linalg.norm(e2, axis=1, keepdims=True)
+    t = e1 + e2
+    n = np.stack([t[:, 1], -t[:, 0]], 1)
+    n /= np.linalg.norm(n, axis=1, keepdims=True)
+    # orient outward: away from the contour's centroid
+    c = np.array([xc.mean(), zc.mean()])
+    if np.sum((np.stack([xc, zc], 1) - c) * n) < 0:
+        n = -n
+    return n[:, 0], n[:, 1]
+
+
+def _ogrid_lines(cx, cz, fx, fz, d, delta):
+    """Grid lines from contour points (cx, cz) to far points (fx, fz) at the
+    distance fractions d: they leave the surface along its normal and turn
+    towards the straight line to the far point over a length ~delta, so the
+    first cells are orthogonal to the wall even at sharp corners."""
+    nx_, nz_ = _contour_normals(cx, cz)
+    L = np.hypot(fx - cx, fz - cz)
+    sx, sz = (fx - cx) / L, (fz - cz) / L
+    dist = d[None, :] * L[:, None]
+    w = np.exp(-dist / delta)
+    dx = w * nx_[:, None] + (1 - w) * sx[:, None]
+    dz = w * nz_[:, None] + (1 - w) * sz[:, None]
+    nrm = np.hypot(dx, dz)
+    X = cx[:, None] + dx / nrm * dist
+    Z = cz[:, None] + dz / nrm * dist
+    return X, Z
+
+
 def airfoil_2d_prisms(n_around: int, n_radial: int, span: float = 0.1, r_far: float = 20.0,
                       first: float = 2e-3) -> ElementMesh:
     """2-D NACA 0012 O-grid, quads cut into 2 triangles, extruded one layer in y.
@@ -329,15 +368,12 @@ def airfoil_2d_prisms(n_around: int, n_radial: int, span: float = 0.1, r_far: fl
     """
     xc, zc = naca0012_contour(n_around)
     centre = np.array([0.5, 0.0])
-    theta = np.arctan2(zc - centre[1], xc - centre[0])
+    theta = 2.0 * math.pi * np.arange(n_around) / n_around     # even far-field angles
     d = _radial(n_radial, first / r_far, 1.0)
     # blend from contour to far circle along each grid line
     far_x = centre[0] + r_far * np.cos(theta)
     far_z = centre[1] + r_far * np.sin(theta)
-    w = d[None, :]
-    # blend with a radius-stretching so near-wall spacing is ~first
-    X2 = xc[:, None] + (far_x - xc)[:, None] * w
-    Z2 = zc[:, None] + (far_z - zc)[:, None] * w
+    X2, Z2 = _ogrid_lines(xc, zc, far_x, far_z, d, 0.1)
     ys = np.array([0.0, span])
     X = np.broadcast_to(X2[:, :, None], (n_around, n_radial + 1, 2))
     Z = np.broadcast_to(Z2[:, :, None], (n_around, n_radial + 1, 2))
@@ -370,115 +406,189 @@ def airfoil_extruded(n_triangles: int) -> ElementMesh:
 
 
 # ---------------------------------------------------------------------------
-# Swept, tapered NACA 0012 semispan wing: prism layers + tets to a far-field
-# hemisphere (truncated by a flat cap), with a rounded tip that closes onto a
-# slit beyond which upper and lower O-grid nodes coincide.
+# Swept, tapered NACA 0012 semispan wing with a flat tip cap: prism layers +
+# tets out to a far-field sphere (truncated by a flat cap).  Beyond the tip
+# the tip section continues spanwise and its interior is filled with a core
+# block of tets, so no cell is degenerate.
 # ---------------------------------------------------------------------------
-def swept_wing(n_around: int = 144, n_radial: int = 37, n_prism: int = 8, n_span_wing: int = 24,
-               n_span_tip: int = 4, n_span_out: int = 12, semispan: float = 1.5, sweep_deg: float = 30.0,
-               taper: float = 0.56, r_far: float = 20.0, first: float = 2e-3) -> ElementMesh:
-    """Semispan wing on the symmetry plane y = 0.
+def naca0012_blunt_contour(n: int) -> Tuple[np.ndarray, np.ndarray]:
+    """O-grid contour of n points (n even) with a blunt trailing edge (the
+    open-TE NACA 0012, base 0.25 % chord): index 0 is the middle of the base,
+    1 the upper TE corner, n/2 the leading edge, n-1 the lower TE corner."""
+    assert n % 2 == 0 and n >= 8
+    half = n // 2
+    beta = np.linspace(0.0, math.pi, half)            # upper corner .. LE: half points
+    x = 0.5 * (1.0 + np.cos(beta))
+    t = 0.6 * (0.2969 * np.sqrt(x) - 0.1260 * x - 0.3516 * x ** 2 + 0.2843 * x ** 3 - 0.1015 * x ** 4)
+    xu, zu = x, t                                      # indices 1 .. half
+    xl, zl = x[::-1][1:-1], -t[::-1][1:-1]             # indices half+1 .. n-1 (LE excluded, corner kept below)
+    xl = np.concatenate([xl, [x[0]]])
+    zl = np.concatenate([zl, [-t[0]]])
+    return np.concatenate([[1.0], xu, xl]), np.concatenate([[0.0], zu, zl])
 
-    Stations are planes y = const: ``n_span_wing`` layers over the wing,
-    ``n_span_tip`` layers over a rounded tip cap of span equal to the tip
-    thickness, and ``n_span_out`` layers beyond, where the section has
-    collapsed onto its chord line (a slit whose upper and lower nodes are
-    shared, so the faces on it are interior).  Each station is an O-grid from
-    the section (or slit) out to the circle where the far-field sphere of
-    radius ``r_far`` cuts the station plane; the last station is a flat cap.
-    Cells: prisms in the first ``n_prism`` radial layers, 6 tets per hex
-    beyond.  Regions: wing, symmetry, farfield.
+
+def _prism_to_tets(b, t, third_from_p: bool) -> np.ndarray:
+    """Split prisms with bottom (s, p, q) = b[:, 0..2], top t[:, 0..2] into 3
+    tets.  The quad faces s-p and s-q are cut from s (bottom) to the top
+    vertex; face p-q from p (bottom) to q' (top) if third_from_p, else from q
+    to p' (the diagonal orientation that avoids a cycle)."""
+    s, p, q = b[:, 0], b[:, 1], b[:, 2]
+    s1, p1, q1 = t[:, 0], t[:, 1], t[:, 2]
+    if third_from_p:
+        tets = [(s, p, q, q1), (s, p, q1, p1), (s, p1, q1, s1)]
+    else:
+        tets = [(s, p, q, p1), (s, q, q1, p1), (s, p1, q1, s1)]
+    return np.stack([np.stack(tt, axis=1) for tt in tets], axis=1).reshape(-1, 4)
+
+
+def _min_angle(p0, p1, p2):
+    """Smallest interior angle of triangles (arrays of 2-D points)."""
+    def ang(a, b, c):
+        u, v = b - a, c - a
+        cosv = np.sum(u * v, -1) / (np.linalg.norm(u, axis=-1) * np.linalg.norm(v, axis=-1))
+        return np.arccos(np.clip(cosv, -1.0, 1.0))
+    return np.minimum(np.minimum(ang(p0, p1, p2), ang(p1, p2, p0)), ang(p2, p0, p1))
+
+
+def _anti_diagonal(X: np.ndarray, Z: np.ndarray) -> np.ndarray:
+    """For the quads of a periodic-in-i structured section grid (X, Z of
+    shape [i, k]), True where the cut (1,0)-(0,1) keeps a larger minimum angle
+    than the cut (0,0)-(1,1)."""
+    P = np.stack([X, Z], axis=-1)
+    p00, p10 = P[:, :-1], np.roll(P, -1, axis=0)[:, :-1]
+    p01, p11 = P[:, 1:], np.roll(P, -1, axis=0)[:, 1:]
+    main = np.minimum(_min_angle(p00, p10, p11), _min_angle(p00, p11, p01))
+    anti = np.minimum(_min_angle(p10, p11, p01), _min_angle(p10, p01, p00))
+    return anti > main
+
+
+def swept_wing(n_around: int = 160, n_radial: int = 48, n_span_wing: int = 40, n_span_out: int = 32,
+               semispan: float = 1.5, sweep_deg: float = 30.0, taper: float = 0.56, r_far: float = 20.0,
+               first: float = 2e-3, tip_cluster: float = 0.5, phi_max_deg: float = 75.0) -> ElementMesh:
+    """Semispan wing on the symmetry plane y = 0 (about 1.1 M cells by default).
+
+    Stations are planes y = const: ``n_span_wing`` layers from the root to the
+    tip (mildly clustered towards the tip) and ``n_span_out`` layers beyond it
+    out to y = 3 semispans, where a flat far-field cap closes the domain.
+    Each station is an O-grid from the section out to the circle where the
+    far-field sphere of radius ``r_far`` cuts the station plane; radial grid
+    lines leave the section along its normal.  Cells are prisms extruded
+    along the span with triangles in the section plane (well shaped from the
+    wall to the far field; wall-parallel triangles or tets cut from the
+    strongly anisotropic hexes give nearly singular least-squares systems).
+    Beyond the flat tip cap the tip section continues as an interior surface
+    that grows with the distance from the tip; inside it is a core of prisms.
+    Regions: wing (surface and tip cap), symmetry, farfield (sphere and cap).
     """
     ni = n_around
     half = ni // 2
-    xc, zc = naca0012_contour(ni)
+    xc, zc = naca0012_contour(ni, cluster=0.5)
     tan_sw = math.tan(math.radians(sweep_deg))
-    c_tip = taper
-    t_tip = 0.12 * c_tip
-    tip_len = t_tip * 0.5
-    y_end = semispan + tip_len
-    y_last = 0.85 * r_far
-    # spanwise stations
-    yw = semispan * (1 - np.cos(np.linspace(0, math.pi / 2, n_span_wing + 1)))      # clustered to tip
-    yt = semispan + tip_len * np.sin(np.linspace(0, math.pi / 2, n_span_tip + 1))[1:]
-    g = _radial(n_span_out, (yw[-1] - yw[-2]) * 1.5, y_last - y_end)[1:]
-    yo = y_end + g
-    ys = np.concatenate([yw, yt, yo])
+    u = np.linspace(0.0, 1.0, n_span_wing + 1)
+    yw = semispan * ((1 - tip_cluster) * u + tip_cluster * np.sin(0.5 * math.pi * u))   # clustered to the tip
+    g = _radial(n_span_out, (yw[-1] - yw[-2]) * 1.2, 2.0 * semispan)[1:]
+    ys = np.concatenate([yw, semispan + g])
     nj = ys.size - 1
-    j_end = n_span_wing + n_span_tip            # first station that is a slit
-    # section scale per station
-    chord = np.where(ys <= semispan, 1.0 - (1.0 - taper) * ys / semispan, c_tip)
+    jt = n_span_wing                                   # tip station
+    chord = np.where(ys <= semispan, 1.0 - (1.0 - taper) * ys / semispan, taper)
     x_le = np.minimum(ys, semispan) * tan_sw
-    thick = np.ones_like(ys)
-    tip_sel = ys > semispan
-    thick[tip_sel] = np.sqrt(np.clip(1.0 - ((ys[tip_sel] - semispan) / tip_len) ** 2, 0.0, 1.0))
-    thick[j_end:] = 0.0
-    # radial distribution (fraction of the way from contour to far circle)
-    d = _radial(n_radial, first / r_far, 1.0)
+    theta = 2.0 * math.pi * np.arange(ni) / ni
+    phi = math.radians(phi_max_deg) * np.arange(nj + 1) / nj
+    x0 = 0.5 * semispan * tan_sw + 0.5
     nk = n_radial
     X = np.empty((ni, nk + 1, nj + 1))
     Y = np.empty_like(X)
     Z = np.empty_like(X)
     for j in range(nj + 1):
-        cx = x_le[j] + chord[j] * xc
-        cz = chord[j] * zc * thick[j]
         ctr_x = x_le[j] + 0.5 * chord[j]
-        r_st = math.sqrt(max(r_far ** 2 - ys[j] ** 2, 1e-12))
-        theta = np.arctan2(chord[j] * zc, cx - ctr_x)
-        fx = ctr_x + r_st * np.cos(theta)
-        fz = r_st * np.sin(theta)
-        X[:, :, j] = cx[:, None] + (fx - cx)[:, None] * d[None, :]
-        Z[:, :, j] = cz[:, None] + (fz - cz)[:, None] * d[None, :]
-        Y[:, :, j] = ys[j]
-    pts = np.stack([X, Y, Z], axis=-1)
-    # node numbering with the slit merge: for j >= j_end, k = 0, node (i) and
-    # (ni - i) are one node.
-    node_index = -np.ones((ni, nk + 1, nj + 1), dtype=np.int64)
-    count = 0
-    flat_pts = []
-    for j in range(nj + 1):
-        for k in range(nk + 1):
-            for_i = np.arange(ni)
-            if j >= j_end and k == 0:
-                own = for_i <= half
-                ids = np.empty(ni, dtype=np.int64)
-                ids[own] = count + np.arange(own.sum())
-                ids[~own] = ids[ni - for_i[~own]]
-                node_index[:, k, j] = ids
-                flat_pts.append(pts[own, k, j])
-                count += int(own.sum())
-            else:
-                node_index[:, k, j] = count + for_i
-                flat_pts.append(pts[:, k, j])
-                count += ni
-    nodes = _f32(np.concatenate(flat_pts))
-    # cells: axes (i around, j span, k radial) so that prisms extrude along k
-    # and lie in the (i, j) wall plane.
-    node_ijk = np.transpose(node_index, (0, 2, 1))            # [i, j, k]
-    ci, cj, ck = np.meshgrid(np.arange(ni), np.arange(nj), np.arange(nk), indexing="ij")
-    cells = np.stack([ci.ravel(), cj.ravel(), ck.ravel()], axis=1)
-    corners = _hex_corner_ids(node_ijk, cells)
-    mirror = cells[:, 0] >= half
-    is_prism = cells[:, 2] < n_prism
-    # SU2 order: prisms first (wall layers), then tets, each in (j, i, k) order
-    order_p = np.lexsort((cells[is_prism, 2], cells[is_prism, 0], cells[is_prism, 1]))
-    order_t = np.lexsort((cells[~is_prism, 2], cells[~is_prism, 0], cells[~is_prism, 1]))
-    prisms = _prisms(corners[is_prism][order_p], mirror[is_prism][order_p])
-    tets = _kuhn_tets(corners[~is_prism][order_t], mirror[~is_prism][order_t])
-    blocks = [(PRISM, prisms), (TET, tets)]
+        cx = x_le[j] + chord[j] * xc
+        cz = chord[j] * zc
+        cy = np.full(ni, ys[j])
+        # far points evenly spaced in longitude theta and latitude phi on the
+        # sphere, so that cells grow in all three directions with the distance
+        fx = x0 + r_far * math.cos(phi[j]) * np.cos(theta)
+        fy = np.full(ni, r_far * math.sin(phi[j]))
+        fz = r_far * math.cos(phi[j]) * np.sin(theta)
+        nx_, nz_ = _contour_normals(cx, cz)
+        L = np.sqrt((fx - cx) ** 2 + (fy - cy) ** 2 + (fz - cz) ** 2)
+        d = _radial(n_radial, first / L.mean(), 1.0)
+        dist = d[None, :] * L[:, None]
+        w = np.exp(-dist / (1.0 * chord[j]))
+        dx = w * nx_[:, None] + (1 - w) * ((fx - cx) / L)[:, None]
+        dy = (1 - w) * ((fy - cy) / L)[:, None]
+        dz = w * nz_[:, None] + (1 - w) * ((fz - cz) / L)[:, None]
+        nrm = np.sqrt(dx * dx + dy * dy + dz * dz)
+        X[:, :, j] = cx[:, None] + dx / nrm * dist
+        Y[:, :, j] = cy[:, None] + dy / nrm * dist
+        Z[:, :, j] = cz[:, None] + dz / nrm * dist
+    n_og = ni * (nk + 1) * (nj + 1)
+    node_index = np.arange(n_og).reshape(nj + 1, nk + 1, ni).transpose(2, 1, 0)   # [i, k, j]
+    pts = np.stack([X, Y, Z], axis=-1).transpose(2, 1, 0, 3).reshape(-1, 3)      # id order (j, k, i)
+    # core mid-thickness nodes for a = 1 .. half-1 at stations j >= jt
+    mid_index = np.full((half, nj + 1), -1, dtype=np.int64)
+    mid_pts = []
+    nxt = n_og
+    for j in range(jt, nj + 1):
+        for a in range(1, half):
+            mid_index[a, j] = nxt
+            nxt += 1
+            mid_pts.append(0.5 * (np.array([X[a, 0, j], Y[a, 0, j], Z[a, 0, j]]) +
+                                  np.array([X[ni - a, 0, j], Y[ni - a, 0, j], Z[ni - a, 0, j]])))
+    nodes = _f32(np.concatenate([pts, np.array(mid_pts).reshape(-1, 3)]))
+    # O-grid cells: hexes (i around, k radial, j span) cut into 2 prisms
+    # extruded along the span, triangles in the section plane.  Each section
+    # quad is cut along the diagonal that keeps the larger minimum angle (at
+    # the root station; the same cut at every station keeps faces shared).
+    ci, ck, cj = np.meshgrid(np.arange(ni), np.arange(nk), np.arange(nj), indexing="ij")
+    order = np.lexsort((ck.ravel(), ci.ravel(), cj.ravel()))            # SU2 order (j, i, k)
+    cells = np.stack([ci.ravel(), ck.ravel(), cj.ravel()], axis=1)[order]
+    corners = _hex_corner_ids(node_index, cells)
+    anti = _anti_diagonal(X[:, :, 0], Z[:, :, 0])                        # [i, k]
+    mirror = anti[cells[:, 0], cells[:, 1]]
+    prisms = [_prisms(corners, mirror)]
+    # core beyond the tip: hexes (a, row, j) for a = 1 .. half-2, rows 0 (upper
+    # to mid) and 1 (mid to lower), cut into 2 span-extruded prisms; the
+    # leading- and trailing-edge fans are one prism per row
+    up = lambda a, j: node_index[a % ni, 0, j]
+    lo = lambda a, j: node_index[(ni - a) % ni, 0, j]
+    col = lambda a, j: (up(a, j), mid_index[a, j], lo(a, j))
+    for j in range(jt, nj):
+        cs = []
+        for a in range(1, half - 1):
+            for row in range(2):
+                c = np.empty((2, 2, 2), dtype=np.int64)     # [a, c, j]
+                for da in range(2):
+                    for dj in range(2):
+                        cc = col(a + da, j + dj)
+                        c[da, 0, dj], c[da, 1, dj] = cc[row], cc[row + 1]
+                cs.append(c)
+        prisms.append(_prisms(np.array(cs)))
+        le, le1 = node_index[half, 0, j], node_index[half, 0, j + 1]
+        te, te1 = node_index[0, 0, j], node_index[0, 0, j + 1]
+        n, n1 = col(half - 1, j), col(half - 1, j + 1)
+        m, m1 = col(1, j), col(1, j + 1)
+        fans = []
+        for r in range(2):
+            fans.append([le, n[r], n[r + 1], le1, n1[r], n1[r + 1]])
+            fans.append([te, m[r], m[r + 1], te1, m1[r], m1[r + 1]])
+        prisms.append(np.array(fans, dtype=np.int64))
+    blocks = [(PRISM, np.concatenate(prisms))]
     # node tags
     kk = np.broadcast_to(np.arange(nk + 1)[None, :, None], node_index.shape)
     jj = np.broadcast_to(np.arange(nj + 1)[None, None, :], node_index.shape)
 
-    def tag(mask):
+    def tag(mask, extra=None):
         t = np.zeros(nodes.shape[0], dtype=bool)
         t[node_index[mask]] = True
+        if extra is not None:
+            t[extra] = True
         return t
 
-    tags = {"wing": tag((kk == 0) & (jj <= j_end)), "symmetry": tag(jj == 0),
-            "farfield": tag((kk == nk) | (jj == nj))}
+    tags = {"wing": tag((kk == 0) & (jj <= jt), mid_index[1:, jt]), "symmetry": tag(jj == 0),
+            "farfield": tag((kk == nk) | (jj == nj), mid_index[1:, nj])}
     markers = _classify(_boundary_faces(blocks), tags)
-    return ElementMesh(nodes, blocks, markers, name=f"swept_wing_{prisms.shape[0] + tets.shape[0]}")
+    n_cells = sum(b.shape[0] for _, b in blocks)
+    return ElementMesh(nodes, blocks, markers, name=f"swept_wing_{n_cells}")
 
 
 def cylinder_ogrid(n_around: int = 400, n_radial: int = 250, ratio: float = 1.03, r_far: float = 30.0,

@@ -484,10 +484,12 @@ struct Solver : SolverBase {
     }
 
     // FvmEulerStepPrepare, src/models/euler.cu:597-647: gradient, limiter
-    // and ghost copy for rho, rhou, rhoe.
-    void prepare() {
+    // and ghost copy for rho, rhou, rhoe; cells [c0, c1) only when c1 > c0
+    // (a bounded sample for timing).
+    void prepare(int64_t c0 = 0, int64_t c1 = -1) {
+        if (c1 < 0) c1 = N;
 #pragma omp parallel for schedule(static)
-        for (int64_t i = 0; i < N; ++i) {
+        for (int64_t i = c0; i < c1; ++i) {
             // ScalarVarComputeGradient / VectorVarComputeGradient, src/fvmops.cu:51-111
             V3<T> gr = mk<T>(0, 0, 0), ge = gr;
             T3<T> gu{gr, gr, gr};
@@ -506,7 +508,7 @@ struct Solver : SolverBase {
             g_rhou[i] = T3<T>{tmul(mat[i], gu.u), tmul(mat[i], gu.v), tmul(mat[i], gu.w)};
         }
 #pragma omp parallel for schedule(static)
-        for (int64_t i = 0; i < N; ++i) {
+        for (int64_t i = c0; i < c1; ++i) {
             // ScalarVarComputeLimiters / VectorVarComputeLimiters, src/fvmops.cu:175-266
             T rmin = rho[i], rmax = rho[i], emin = rhoe[i], emax = rhoe[i];
             V3<T> umin = rhou[i], umax = rhou[i];
@@ -547,10 +549,12 @@ struct Solver : SolverBase {
     }
 
     // fvmEulerSteadyOp + euler_steady_step, src/models/euler.cu:236-381,
-    // with a Jacobi update into the *_n arrays.
-    void step(T cfl) {
+    // with a Jacobi update into the *_n arrays; cells [b0, b1) only when
+    // b1 > b0.
+    void step(T cfl, int64_t b0 = 0, int64_t b1 = -1) {
+        if (b1 < 0) b1 = N;
 #pragma omp parallel for schedule(static)
-        for (int64_t c0 = 0; c0 < N; ++c0) {
+        for (int64_t c0 = b0; c0 < b1; ++c0) {
             T dt = 0, fr = 0, fe = 0;
             V3<T> fu = mk<T>(0, 0, 0);
             const T v = cv[c0];
@@ -589,7 +593,7 @@ struct Solver : SolverBase {
             rhoe_n[c0] = rhoe[c0] - fe * dt;
             err[c0] = (fr * fr + dot(fu, fu) + fe * fe) * v;
         }
-        for (int64_t c = 0; c < N; ++c) { rho[c] = rho_n[c]; rhou[c] = rhou_n[c]; rhoe[c] = rhoe_n[c]; }
+        for (int64_t c = b0; c < b1; ++c) { rho[c] = rho_n[c]; rhou[c] = rhou_n[c]; rhoe[c] = rhoe_n[c]; }
     }
 
     // FvmFieldReduceSum, src/fvmops.cu:369-383 (accumulated in double here)
@@ -787,6 +791,18 @@ void orc_step(void* hp, double cfl) {
 double orc_reduce_error(void* hp) {
     Handle* h = static_cast<Handle*>(hp);
     return dispatch(h->s, h->bits, [&](auto* s) { return s->reduce_error(); });
+}
+
+// Gradients/limiters and the flux/update for the interior cells [c0, c1)
+// only: a bounded sample of one iteration, for CPU timing.
+void orc_sample_step(void* hp, double cfl, int64_t c0, int64_t c1) {
+    Handle* h = static_cast<Handle*>(hp);
+    dispatch(h->s, h->bits, [&](auto* s) {
+        using T = std::remove_reference_t<decltype(s->rho[0])>;
+        s->prepare(c0, c1);
+        s->step((T)cfl, c0, c1);
+        return 0;
+    });
 }
 
 // The PhysicsEuler::step loop (src/models/euler.cu:99-175) for n_iter

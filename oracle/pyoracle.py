@@ -53,6 +53,7 @@ def load():
     lib.orc_reduce_error.restype = _D
     lib.orc_reduce_error.argtypes = [_P]
     lib.orc_run.argtypes = [_P, _I64, _D, _I64, _P, _P, _P, _P]
+    lib.orc_sample_step.argtypes = [_P, _D, _I64, _I64]
     _lib = lib
     return lib
 
@@ -179,6 +180,10 @@ class OracleSolver:
 
     def reduce_error(self) -> float:
         return float(load().orc_reduce_error(self.h))
+
+    def sample_step(self, cfl: float, c0: int, c1: int) -> None:
+        """Gradients, limiters and flux/update of interior cells [c0, c1)."""
+        load().orc_sample_step(self.h, cfl, c0, c1)
 
     def run(self, bcs, n_iter: int, cfl: float) -> np.ndarray:
         types = np.array([0 if b[0] == "slip" else 1 for b in bcs], dtype=np.int32)

@@ -38,13 +38,24 @@ def test_airfoil_sizes():
 
 
 def test_swept_wing_small_is_valid():
-    """Prism layers + tets with the collapsed tip slit: a conforming mesh with
-    positive volumes and three boundary regions."""
-    m = meshgen.swept_wing(n_around=24, n_radial=8, n_prism=2, n_span_wing=4, n_span_tip=2, n_span_out=3)
+    """Span-extruded prisms around the wing and the core beyond the tip: a
+    conforming mesh (the oracle's converter checks that every face has two
+    cells) with positive volumes, three boundary regions and well-conditioned
+    least-squares systems."""
+    m = meshgen.swept_wing(n_around=24, n_radial=8, n_span_wing=4, n_span_out=3)
     om = OracleMesh(m)
     assert set(m.markers) == {"wing", "symmetry", "farfield"}
     vol = om.get("cell_volumes")[: om.N]
     assert vol.min() > 0
+    N = om.N
+    cfs, cc = om.get("cell_faces_starts"), om.get("cell_connects")
+    c = om.get("cell_centers").reshape(-1, 3)
+    owner = np.repeat(np.arange(N), np.diff(cfs[: N + 1]))
+    d = c[cc[: cfs[N]]] - c[owner]
+    u = d / np.linalg.norm(d, axis=1, keepdims=True)
+    a = np.zeros((N, 3, 3))
+    np.add.at(a, owner, u[:, :, None] * u[:, None, :])
+    assert np.linalg.eigvalsh(a)[:, 0].min() > 1e-3
     # the symmetry plane is flat at y = 0
     sym = np.concatenate([c.reshape(-1) for _, c in m.markers["symmetry"]])
     assert np.allclose(m.nodes[sym, 1], 0.0)
