@@ -16,6 +16,17 @@
 namespace gb {
 namespace {
 
+// Resident blocks per SM the two hot kernels are compiled for (register
+// budget 65536 / (kBlock * blocks)).
+#ifndef GB_FLUX_BLOCKS
+#define GB_FLUX_BLOCKS 3
+#endif
+#ifndef GB_GRAD_BLOCKS
+#define GB_GRAD_BLOCKS 4
+#endif
+constexpr int kFluxBlocksPerSM = GB_FLUX_BLOCKS;
+constexpr int kGradBlocksPerSM = GB_GRAD_BLOCKS;
+
 __device__ __forceinline__ float3 f3(float4 a) { return make_float3(a.x, a.y, a.z); }
 __device__ __forceinline__ float3 operator+(float3 a, float3 b) { return make_float3(a.x + b.x, a.y + b.y, a.z + b.z); }
 __device__ __forceinline__ float3 operator-(float3 a, float3 b) { return make_float3(a.x - b.x, a.y - b.y, a.z - b.z); }
@@ -156,7 +167,7 @@ __global__ void k_bc_farfield(uint32_t g0, uint32_t g1, uint32_t N, const float4
 // Fused FvmEulerStepPrepare (src/models/euler.cu:597-647): least-squares
 // gradients (src/fvmops.cu:51-111) and limiters (src/fvmops.cu:175-266) of
 // rho, rhou (3 components) and rhoE in one pass over each cell's faces.
-__global__ void __launch_bounds__(kBlock) k_grad_lim(uint32_t N, const float4* __restrict__ cell_geo,
+__global__ void __launch_bounds__(kBlock, kGradBlocksPerSM) k_grad_lim(uint32_t N, const float4* __restrict__ cell_geo,
                                                     const float4* __restrict__ face_geo,
                                                     const uint32_t* __restrict__ start, const uint2* __restrict__ nb,
                                                     const float4* __restrict__ lsq, EulerState q, EulerGrad g) {
@@ -249,7 +260,7 @@ __device__ __forceinline__ void reconstruct(float r, float4 u, float e, float4 g
 // dt = cfl / sum, q_new = q - F dt (into the other buffer), and the squared
 // residual (F_rho^2 + |F_rhou|^2 + F_rhoE^2) V, summed per block in float64.
 template <bool TRANSPOSED>
-__global__ void __launch_bounds__(kBlock) k_flux(uint32_t N, const float4* __restrict__ cell_geo,
+__global__ void __launch_bounds__(kBlock, kFluxBlocksPerSM) k_flux(uint32_t N, const float4* __restrict__ cell_geo,
                                                 const float4* __restrict__ face_geo,
                                                 const uint32_t* __restrict__ start, const uint2* __restrict__ nb,
                                                 EulerState q, const float4* __restrict__ g_rho,
@@ -299,16 +310,19 @@ __global__ void __launch_bounds__(kBlock) k_flux(uint32_t N, const float4* __res
             float3 ua, ub;
             reconstruct<TRANSPOSED>(r0, u0, e0, gr0, gu0, ge0, d0, ra, ua, ea);
             reconstruct<TRANSPOSED>(r1, u1, e1, gr1, gu1, ge1, d1, rb, ub, eb);
-            const float pa = 0.4f * (ea - 0.5f / ra * dot(ua, ua));
-            const float pb = 0.4f * (eb - 0.5f / rb * dot(ub, ub));
-            const float va = dot(ua, n) / ra;
-            const float vb = dot(ub, n) / rb;
+            // one reciprocal of the density per side, reused by every quotient
+            const float ia = 1.f / ra, ib = 1.f / rb;
+            const float qa = dot(ua, ua), qb = dot(ub, ub);
+            const float pa = 0.4f * (ea - 0.5f * ia * qa);
+            const float pb = 0.4f * (eb - 0.5f * ib * qb);
+            const float va = dot(ua, n) * ia;
+            const float vb = dot(ub, n) * ib;
             const float h = ds * 0.5f;
             fr += (va * ra + vb * rb) * h;
             fu = fu + ((ua * va + n * pa) + (ub * vb + n * pb)) * h;
             fe += (va * (ea + pa) + vb * (eb + pb)) * h;
-            const float eig = fmaxf(norm(ua * (1.f / ra)) + lsqrt(1.4f * pa / ra),
-                                    norm(ub * (1.f / rb)) + lsqrt(1.4f * pb / rb));
+            const float eig = fmaxf(sqrtf(qa) * ia + lsqrt(1.4f * pa * ia),
+                                    sqrtf(qb) * ib + lsqrt(1.4f * pb * ib));
             const float eh = eig * h;
             fr -= eh * (rb - ra);
             fu = fu - (ub - ua) * eh;
