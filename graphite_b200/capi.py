@@ -97,6 +97,7 @@ _PROTOS = {
     "gbEulerRun": (C.c_int64, [MeshP, FieldP, FieldP, FieldP, FieldP, C.c_float, C.c_int64, C.POINTER(gbBc), C.c_int,
                                C.c_double, C.c_int, C.POINTER(C.c_double)]),
     "gbKernelLaunchCount": (C.c_uint64, []),
+    "gbReduceSumNoAlloc": (C.c_int, [C.c_void_p, C.c_uint64, C.c_void_p, C.c_void_p]),
 }
 
 _lib = None

@@ -440,6 +440,11 @@ void launch_reduce_partials(int64_t n, const float* v, double* partials, cudaStr
     count_launch();
 }
 
+void launch_reduce_partials_blocks(int64_t n, const float* v, double* partials, int blocks, cudaStream_t s) {
+    k_reduce_partials<<<blocks, kBlock, 0, s>>>(n, v, partials);
+    count_launch();
+}
+
 void launch_reduce_final(int n_partials, const double* partials, double* out, double* history,
                          unsigned long long* counter, cudaStream_t s) {
     k_reduce_final<<<1, kBlock, 0, s>>>(n_partials, partials, out, history, counter);

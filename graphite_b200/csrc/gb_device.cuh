@@ -76,6 +76,8 @@ void launch_grad_lim(const DevMesh& m, EulerState q, EulerGrad g, cudaStream_t s
 void launch_flux(const DevMesh& m, EulerState q, EulerGrad g, float* rho_n, float4* rhou_n, float* rhoe_n,
                  float* err, double* partials, float cfl, bool transposed, cudaStream_t s);
 void launch_reduce_partials(int64_t n, const float* v, double* partials, cudaStream_t s);
+// stage 1 with a caller-chosen number of blocks (one partial per block)
+void launch_reduce_partials_blocks(int64_t n, const float* v, double* partials, int blocks, cudaStream_t s);
 void launch_reduce_final(int n_partials, const double* partials, double* out, double* history,
                          unsigned long long* counter, cudaStream_t s);
 
