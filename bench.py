@@ -304,6 +304,11 @@ def run_ours(args, rank, world, local_rank):
                "min_residual_ratio": float(np.min(ratio)), "max_iterations": args.max_iters,
                "metric": "sum over cells of (F_rho^2+|F_rhou|^2+F_rhoE^2) V, relative to iteration 0"}
 
+    # ---- batched sweep (config 3), optional ----
+    batch = None
+    if rank == 0 and args.batch:
+        batch = run_batch_comparison(args, dev_stream)
+
     # ---- CPU baseline (rank 0, N = 1) ----
     cpu = None
     if rank == 0 and world == 1 and not args.skip_cpu:
@@ -330,6 +335,7 @@ def run_ours(args, rank, world, local_rank):
         "clocks": clocks.summary(),
         "residual_finite": finite,
         "time_to_1e-3": ttr,
+        "batched_airfoil_sweep": batch,
         "cpu_baseline": cpu,
     }
     case.close()
@@ -371,6 +377,104 @@ def cpu_baseline(workload, max_seconds=20.0, sample_cells=None):
     return {"value": done / dt, "unit": "cell-updates/s", "cores": po.max_threads(), "kind": "port",
             "sample": f"{done} cell-updates in blocks of {block} cells of the {N}-cell mesh over {dt:.1f} s "
                       "(gradients, limiters, flux and update; float32)"}
+
+
+AIRFOIL_SET = ((50_000, 24), (120_000, 24), (300_000, 16))
+BATCH_SEED = 20261203
+# CFL of the reference's own airfoil example (examples/airfoil/airfoil.json);
+# the explicit scheme's residual stalls above 1e-3 on the finer meshes at 0.8
+SWEEP_CFL = 0.5
+SWEEP_MAX_ITERS = 20000
+
+
+def airfoil_instances(seed=BATCH_SEED, aoa_range=(-2.0, 6.0)):
+    """(mesh index, Mach, AoA deg) for the 64 seeded instances of the batched
+    airfoil sweep: Mach ~ U[0.3, 0.8], AoA ~ U[-2, 6] deg."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for mi, (_, count) in enumerate(AIRFOIL_SET):
+        for _ in range(count):
+            out.append((mi, float(rng.uniform(0.3, 0.8)), float(rng.uniform(*aoa_range))))
+    return out
+
+
+def airfoil_case(mach, aoa_deg):
+    a = math.radians(aoa_deg)
+    m = (mach * math.cos(a), 0.0, mach * math.sin(a))
+    bcs = [("farfield", "farfield") + m + (P_INF, T_INF), ("slip", "sides"), ("slip", "wing")]
+    return m, bcs
+
+
+def run_batch_comparison(args, dev_stream):
+    """Config 3: 64 instances of the extruded NACA 0012 airfoil on the 50k,
+    120k and 300k meshes, each to a 1e-3 residual drop; sequential plain
+    solves (gbEulerRun per instance) versus one batched, autotuned solve."""
+    import torch
+    from graphite_b200 import meshgen
+    from graphite_b200.batch import EulerBatch
+    from graphite_b200.euler import EulerCase
+
+    cache = os.path.join(tempfile.gettempdir(), "graphite_b200_bench")
+    os.makedirs(cache, exist_ok=True)
+    cases_ = []
+    for n_tri, _ in AIRFOIL_SET:
+        path = os.path.join(cache, f"airfoil_{n_tri}.su2")
+        if not os.path.exists(path):
+            tmp = path + f".tmp{os.getpid()}"
+            meshgen.airfoil_extruded(n_tri).write_su2(tmp)
+            os.replace(tmp, path)
+        cases_.append(EulerCase(path))
+    inst = airfoil_instances()
+    tol, cap, cfl = 1e-3, SWEEP_MAX_ITERS, SWEEP_CFL
+    ev = lambda: torch.cuda.Event(enable_timing=True)
+    # plain: one gbEulerRun per instance, back to back
+    plain_iters, plain_ms = [], 0.0
+    for mi, mach, aoa in inst:
+        m, bcs = airfoil_case(mach, aoa)
+        c = cases_[mi]
+        c.init(m, P_INF, T_INF)
+        e0, e1 = ev(), ev()
+        torch.cuda.synchronize()
+        e0.record(dev_stream)
+        h = c.run(bcs, cfl, cap, tolerance=tol, check_every=100)
+        e1.record(dev_stream)
+        torch.cuda.synchronize()
+        plain_ms += e0.elapsed_time(e1)
+        r = h / h[0]
+        plain_iters.append(int(np.argmax(r < tol)) + 1 if np.any(r < tol) else len(h))
+    spec = [(mi, airfoil_case(mach, aoa)[1]) for mi, mach, aoa in inst]
+    with EulerBatch(cases_, spec) as b:
+        for i, (mi, mach, aoa) in enumerate(inst):
+            b.init_uniform(i, airfoil_case(mach, aoa)[0], P_INF, T_INF)
+        t0 = time.perf_counter()
+        tile, sched = b.autotune(cfl, trial_iters=5)
+        tune_s = time.perf_counter() - t0
+        for i, (mi, mach, aoa) in enumerate(inst):
+            b.init_uniform(i, airfoil_case(mach, aoa)[0], P_INF, T_INF)
+        e0, e1 = ev(), ev()
+        torch.cuda.synchronize()
+        e0.record(dev_stream)
+        done, its, rat, st = b.run(cfl, cap, tolerance=tol, check_every=100)
+        e1.record(dev_stream)
+        torch.cuda.synchronize()
+        batch_ms = e0.elapsed_time(e1)
+    for c in cases_:
+        c.close()
+    cells = [cases_[mi].n_cells for mi, _, _ in inst]
+    upd_plain = float(sum(c * k for c, k in zip(cells, plain_iters)))
+    upd_batch = float(sum(c * int(k) for c, k in zip(cells, its)))
+    return {
+        "instances": len(inst), "meshes": [n for n, _ in AIRFOIL_SET], "per_mesh": [c for _, c in AIRFOIL_SET],
+        "tolerance": tol, "seed": BATCH_SEED, "cfl": cfl, "max_iterations": cap,
+        "plain": {"seconds": plain_ms * 1e-3, "seconds_per_case": plain_ms * 1e-3 / len(inst),
+                  "cell_updates_per_s": upd_plain / (plain_ms * 1e-3), "iterations": plain_iters,
+                  "converged": int(sum(1 for k in plain_iters if k < cap))},
+        "batched": {"seconds": batch_ms * 1e-3, "seconds_per_case": batch_ms * 1e-3 / len(inst),
+                    "cell_updates_per_s": upd_batch / (batch_ms * 1e-3), "iterations": [int(k) for k in its],
+                    "converged": int(np.sum(st == 1)), "tile_cells": tile, "schedule": sched,
+                    "autotune_seconds": tune_s},
+        "speedup_per_case": plain_ms / batch_ms,
+    }
 
 
 def run_reference(args, rank, world):
@@ -425,6 +529,7 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--skip-convergence", action="store_true")
+    ap.add_argument("--batch", action="store_true", help="also run the batched 64-instance airfoil sweep")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -61,6 +61,10 @@ class gbBc(C.Structure):
                 ("temperature", C.c_float)]
 
 
+class gbBatchInstance(C.Structure):
+    _fields_ = [("mesh", C.c_int), ("n_bc", C.c_int), ("bcs", C.POINTER(gbBc))]
+
+
 MeshP = C.POINTER(cuMesh)
 FieldP = C.POINTER(FvmField)
 
@@ -98,6 +102,16 @@ _PROTOS = {
                                C.c_double, C.c_int, C.POINTER(C.c_double)]),
     "gbKernelLaunchCount": (C.c_uint64, []),
     "gbReduceSumNoAlloc": (C.c_int, [C.c_void_p, C.c_uint64, C.c_void_p, C.c_void_p]),
+    "gbBatchCreate": (C.c_void_p, [C.c_int, C.POINTER(MeshP), C.c_int, C.POINTER(gbBatchInstance)]),
+    "gbBatchFree": (None, [C.c_void_p]),
+    "gbBatchInitUniform": (C.c_int, [C.c_void_p, C.c_int, gb_vector, C.c_float, C.c_float]),
+    "gbBatchSetState": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "gbBatchGetState": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "gbBatchSetTuning": (C.c_int, [C.c_void_p, C.c_int, C.c_int]),
+    "gbBatchGetTuning": (C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+    "gbBatchAutotune": (C.c_int, [C.c_void_p, C.c_float, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+    "gbBatchRun": (C.c_int64, [C.c_void_p, C.c_float, C.c_int64, C.c_double, C.c_int, C.POINTER(C.c_int64),
+                               C.POINTER(C.c_double), C.POINTER(C.c_int), C.POINTER(C.c_double)]),
 }
 
 _lib = None

@@ -387,6 +387,21 @@ bool download_gradients(FvmField* f) {
 }
 
 }  // namespace
+
+bool mesh_access(cuMesh* mesh, MeshAccess* out) {
+    MeshImpl* mi = impl(mesh);
+    if (!mi) { set_error("null mesh"); return false; }
+    out->dev = &mi->dev;
+    out->d_cell_new = mi->d_cell_new;
+    out->region_start = mi->num.region_start.data();
+    out->n_regions = (int)mi->topo.regions.size();
+    out->N = mi->topo.N;
+    out->G = mi->topo.G;
+    return true;
+}
+
+bool reference_momentum() { return g_transposed.load() != 0; }
+
 }  // namespace gb
 
 using namespace gb;

@@ -1,0 +1,651 @@
+// Batched multi-instance Euler solver: many (mesh, Mach, AoA) instances on
+// meshes of uneven sizes advanced together.
+//
+// Each iteration is four kernels that each cover every active instance --
+// boundary ghosts, gradients + limiters, flux + update, and a
+// per-instance residual reduction that also flips the instance's value
+// buffer and freezes it once its residual ratio drops below the tolerance --
+// captured in a CUDA graph and replayed.  Work is a list of (instance, tile
+// of cells) items, one block each; the list holds the active instances only
+// (it is rebuilt when instances freeze), and its order (the "schedule") and
+// the tile size are picked by an autotuner.  In tile-major order the instances that share a mesh process
+// the same tile back to back, so the mesh data of that tile is read from HBM
+// once and reused from L2 by the other instances.
+//
+// The per-cell arithmetic is the single-mesh path's (euler_ops.cuh), summed
+// in the same order; the residual of each instance is reduced in a fixed
+// order, so every instance follows the same iterates as a plain solve of it.
+#include <algorithm>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "euler_ops.cuh"
+#include "gb_internal.h"
+
+namespace gb {
+namespace {
+
+constexpr int kMaxRegions = 16;
+constexpr int kGhostTile = kBlock;
+
+struct InstDev {
+    float* rho[2];
+    float4* rhou[2];
+    float* rhoe[2];
+    float4* g_rho;
+    float4* g_rhou;
+    float4* g_rhoe;
+    double* partials;     // one per cell tile
+    double* hist;         // residual per iteration of the current run
+    int mesh;
+    int n_tiles;
+    int cur;
+    int status;           // 0 running, 1 converged, 2 iteration cap, 3 not finite
+    int iters;
+    int max_iter;
+    double res0;
+    double ratio;
+    int bc[kMaxRegions];  // boundary condition per region (index into the BC table), -1 none
+};
+
+struct MeshTab {
+    MeshDev m;
+    const uint2* ghost;
+    const uint8_t* ghost_region;
+    uint32_t G;
+};
+
+struct BcDev {
+    int type;             // 0 slip, 1 far field
+    float3 mach;
+    float p, t;
+};
+
+// Two register budgets for the batched gradient / flux kernels (resident
+// 256-thread blocks per SM): variant 0 keeps every value in registers,
+// variant 1 trades a few spills for one more resident block.  The autotuner
+// picks one.
+constexpr int kBatchGradBlocks[2] = {3, 4};
+constexpr int kBatchFluxBlocks[2] = {2, 3};
+
+__global__ void k_batch_bc(const int2* __restrict__ items, int n_items, InstDev* insts,
+                           const MeshTab* __restrict__ meshes, const BcDev* __restrict__ bcs) {
+    for (int it = blockIdx.x; it < n_items; it += gridDim.x) {
+        const int2 w = items[it];
+        const InstDev& I = insts[w.x];
+        if (I.status) continue;
+        const MeshTab& M = meshes[I.mesh];
+        const uint32_t g = (uint32_t)w.y * kGhostTile + threadIdx.x;
+        if (g >= M.G) continue;
+        const int b = I.bc[M.ghost_region[g]];
+        if (b < 0) continue;
+        const int cur = I.cur;
+        const BcDev bc = bcs[b];
+        float r, e;
+        float4 ru;
+        if (bc.type == 0)
+            slip_ghost(M.m.cell_geo, M.m.face_geo, M.ghost[g], I.rho[cur], I.rhou[cur], I.rhoe[cur], r, ru, e);
+        else
+            farfield_ghost(M.m.cell_geo, M.m.face_geo, M.ghost[g], I.rho[cur], I.rhou[cur], I.rhoe[cur], bc.mach,
+                           bc.p, bc.t, r, ru, e);
+        const uint32_t t = M.m.N + g;
+        for (int k = 0; k < 2; ++k) {
+            I.rho[k][t] = r;
+            I.rhou[k][t] = ru;
+            I.rhoe[k][t] = e;
+        }
+    }
+}
+
+template <int BLOCKS>
+__global__ void __launch_bounds__(kBlock, BLOCKS)
+    k_batch_grad(const int2* __restrict__ items, const InstDev* insts, const MeshTab* __restrict__ meshes, int tile) {
+    const int2 w = items[blockIdx.x];
+    const InstDev& I = insts[w.x];
+    if (I.status) return;
+    const MeshDev m = meshes[I.mesh].m;
+    const int cur = I.cur;
+    const EulerState q{I.rho[cur], I.rhou[cur], I.rhoe[cur]};
+    const EulerGrad g{I.g_rho, I.g_rhou, I.g_rhoe};
+    const uint32_t c0 = (uint32_t)w.y * tile;
+    const uint32_t c1 = min(m.N, c0 + (uint32_t)tile);
+    for (uint32_t i = c0 + threadIdx.x; i < c1; i += blockDim.x) grad_lim_cell(m, q, g, i);
+}
+
+template <bool TRANSPOSED, int BLOCKS>
+__global__ void __launch_bounds__(kBlock, BLOCKS)
+    k_batch_flux(const int2* __restrict__ items, const InstDev* insts, const MeshTab* __restrict__ meshes, int tile,
+                 float cfl) {
+    const int2 w = items[blockIdx.x];
+    const InstDev& I = insts[w.x];
+    if (I.status) return;                     // uniform over the block
+    const MeshDev m = meshes[I.mesh].m;
+    const int cur = I.cur, nxt = 1 - I.cur;
+    const EulerState q{I.rho[cur], I.rhou[cur], I.rhoe[cur]};
+    const uint32_t c0 = (uint32_t)w.y * tile;
+    const uint32_t c1 = min(m.N, c0 + (uint32_t)tile);
+    double res = 0.0;
+    for (uint32_t i = c0 + threadIdx.x; i < c1; i += blockDim.x)
+        res += (double)flux_cell<TRANSPOSED>(m, q, I.g_rho, I.g_rhou, I.g_rhoe, I.rho[nxt], I.rhou[nxt], I.rhoe[nxt],
+                                             nullptr, cfl, i);
+    const double bs = block_sum(res);
+    if (threadIdx.x == 0) I.partials[w.y] = bs;
+}
+
+__global__ void k_batch_reduce(InstDev* insts, double tol) {
+    InstDev& I = insts[blockIdx.x];
+    if (I.status) return;
+    double s = 0.0;
+    for (int k = threadIdx.x; k < I.n_tiles; k += blockDim.x) s += I.partials[k];
+    const double bs = block_sum(s);
+    if (threadIdx.x == 0) {
+        if (I.iters == 0) I.res0 = bs;
+        const double ratio = I.res0 > 0.0 ? bs / I.res0 : 0.0;
+        if (I.hist) I.hist[I.iters] = bs;
+        I.iters += 1;
+        I.ratio = ratio;
+        I.cur ^= 1;
+        if (!(bs == bs) || bs > 1e300) I.status = 3;
+        else if (tol > 0.0 && ratio < tol) I.status = 1;
+        else if (I.iters >= I.max_iter) I.status = 2;
+    }
+}
+
+int sm_count() {
+    static int n = 0;
+    if (!n) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+        if (n <= 0) n = 148;
+    }
+    return n;
+}
+
+}  // namespace
+}  // namespace gb
+
+struct gbBatchImpl {
+    std::vector<cuMesh*> meshes;
+    std::vector<gb::MeshAccess> acc;
+    std::vector<uint8_t*> d_ghost_region;
+    gb::MeshTab* d_mesh = nullptr;
+    int n_inst = 0;
+    std::vector<gb::InstDev> h_inst;
+    gb::InstDev* d_inst = nullptr;
+    std::vector<gb::BcDev> h_bcs;
+    gb::BcDev* d_bcs = nullptr;
+    int tile = gb::kBlock;
+    int schedule = 1;     // 0 instance-major, 1 tile-major
+    int variant = 0;      // register budget of the gradient/flux kernels
+    int2* d_cell_items = nullptr;
+    int n_cell_items = 0;
+    int2* d_ghost_items = nullptr;
+    int n_ghost_items = 0;
+    std::vector<void*> allocations;
+    std::string signature;
+};
+
+namespace gb {
+using Batch = ::gbBatchImpl;
+
+namespace {
+
+struct Tuning {
+    int tile, schedule, variant;
+};
+std::map<std::string, Tuning> g_tuning_cache;
+
+bool ok_(cudaError_t e, const char* what) {
+    if (e == cudaSuccess) return true;
+    set_error(std::string(what) + ": " + cudaGetErrorString(e));
+    return false;
+}
+
+template <typename T>
+bool balloc(Batch* b, T*& p, size_t n, const char* what) {
+    p = nullptr;
+    if (!ok_(cudaMalloc((void**)&p, std::max<size_t>(n, 1) * sizeof(T)), what)) return false;
+    b->allocations.push_back((void*)p);
+    return true;
+}
+
+int64_t tiles_of(const Batch* b, int inst, int tile) {
+    const int64_t N = b->acc[b->h_inst[inst].mesh].N;
+    return (N + tile - 1) / tile;
+}
+
+bool build_items(Batch* b) {
+    std::vector<int2> items;
+    auto active = [&](int i) { return b->h_inst[i].status == 0; };
+    if (b->schedule == 0) {
+        for (int i = 0; i < b->n_inst; ++i)
+            if (active(i))
+                for (int64_t t = 0; t < tiles_of(b, i, b->tile); ++t) items.push_back(make_int2(i, (int)t));
+    } else {
+        // tile-major within each mesh: instances that share a mesh take the
+        // same tile back to back
+        for (size_t m = 0; m < b->meshes.size(); ++m) {
+            std::vector<int> insts;
+            for (int i = 0; i < b->n_inst; ++i)
+                if (b->h_inst[i].mesh == (int)m && active(i)) insts.push_back(i);
+            if (insts.empty()) continue;
+            const int64_t nt = (b->acc[m].N + b->tile - 1) / b->tile;
+            for (int64_t t = 0; t < nt; ++t)
+                for (int i : insts) items.push_back(make_int2(i, (int)t));
+        }
+    }
+    std::vector<int2> gitems;
+    for (int i = 0; i < b->n_inst; ++i) {
+        if (!active(i)) continue;
+        const int64_t G = b->acc[b->h_inst[i].mesh].G;
+        for (int64_t t = 0; t * kGhostTile < G; ++t) gitems.push_back(make_int2(i, (int)t));
+    }
+    if (b->d_cell_items) cudaFree(b->d_cell_items);
+    if (b->d_ghost_items) cudaFree(b->d_ghost_items);
+    b->d_cell_items = nullptr;
+    b->d_ghost_items = nullptr;
+    b->n_cell_items = (int)items.size();
+    b->n_ghost_items = (int)gitems.size();
+    if (!ok_(cudaMalloc((void**)&b->d_cell_items, std::max<size_t>(items.size(), 1) * sizeof(int2)), "batch items") ||
+        !ok_(cudaMalloc((void**)&b->d_ghost_items, std::max<size_t>(gitems.size(), 1) * sizeof(int2)), "batch items"))
+        return false;
+    cudaStream_t s = (cudaStream_t)gbGetStream();
+    return ok_(cudaMemcpyAsync(b->d_cell_items, items.data(), items.size() * sizeof(int2), cudaMemcpyHostToDevice, s),
+               "batch items") &&
+           ok_(cudaMemcpyAsync(b->d_ghost_items, gitems.data(), gitems.size() * sizeof(int2), cudaMemcpyHostToDevice, s),
+               "batch items");
+}
+
+// partial-sum buffers sized for the current tile
+bool size_partials(Batch* b) {
+    for (int i = 0; i < b->n_inst; ++i) {
+        InstDev& I = b->h_inst[i];
+        const int64_t nt = tiles_of(b, i, b->tile);
+        if (I.partials && nt <= I.n_tiles) { I.n_tiles = (int)nt; continue; }
+        double* p = nullptr;
+        if (!balloc(b, p, (size_t)std::max<int64_t>(nt, tiles_of(b, i, kBlock)), "batch partials")) return false;
+        I.partials = p;
+        I.n_tiles = (int)nt;
+    }
+    return true;
+}
+
+bool upload_inst(Batch* b) {
+    return ok_(cudaMemcpyAsync(b->d_inst, b->h_inst.data(), b->h_inst.size() * sizeof(InstDev), cudaMemcpyHostToDevice,
+                               (cudaStream_t)gbGetStream()),
+               "batch table");
+}
+
+bool download_inst(Batch* b) {
+    cudaStream_t s = (cudaStream_t)gbGetStream();
+    return ok_(cudaMemcpyAsync(b->h_inst.data(), b->d_inst, b->h_inst.size() * sizeof(InstDev), cudaMemcpyDeviceToHost,
+                               s),
+               "batch table") &&
+           ok_(cudaStreamSynchronize(s), "batch table");
+}
+
+void enqueue_iteration(Batch* b, float cfl, double tol, cudaStream_t s) {
+    const int gb_items = std::min(b->n_ghost_items, sm_count() * 8);
+    if (b->n_ghost_items)
+        k_batch_bc<<<gb_items, kGhostTile, 0, s>>>(b->d_ghost_items, b->n_ghost_items, b->d_inst, b->d_mesh, b->d_bcs);
+    if (b->n_cell_items) {
+        const int n = b->n_cell_items;
+        const bool tr = reference_momentum();
+        if (b->variant == 0) {
+            k_batch_grad<kBatchGradBlocks[0]><<<n, kBlock, 0, s>>>(b->d_cell_items, b->d_inst, b->d_mesh, b->tile);
+            if (tr) k_batch_flux<true, kBatchFluxBlocks[0]><<<n, kBlock, 0, s>>>(b->d_cell_items, b->d_inst, b->d_mesh, b->tile, cfl);
+            else k_batch_flux<false, kBatchFluxBlocks[0]><<<n, kBlock, 0, s>>>(b->d_cell_items, b->d_inst, b->d_mesh, b->tile, cfl);
+        } else {
+            k_batch_grad<kBatchGradBlocks[1]><<<n, kBlock, 0, s>>>(b->d_cell_items, b->d_inst, b->d_mesh, b->tile);
+            if (tr) k_batch_flux<true, kBatchFluxBlocks[1]><<<n, kBlock, 0, s>>>(b->d_cell_items, b->d_inst, b->d_mesh, b->tile, cfl);
+            else k_batch_flux<false, kBatchFluxBlocks[1]><<<n, kBlock, 0, s>>>(b->d_cell_items, b->d_inst, b->d_mesh, b->tile, cfl);
+        }
+    }
+    k_batch_reduce<<<b->n_inst, kBlock, 0, s>>>(b->d_inst, tol);
+}
+
+// Runs up to max_iter iterations (graph replay, status polled every
+// check_every); per-instance state lives in d_inst.
+int64_t run_loop(Batch* b, float cfl, int64_t max_iter, double tol, int check_every) {
+    cudaStream_t s = (cudaStream_t)gbGetStream();
+    cudaStream_t cap = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    bool ok = ok_(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking), "batch graph");
+    auto capture = [&]() {
+        if (exec) cudaGraphExecDestroy(exec);
+        exec = nullptr;
+        cudaGraph_t graph = nullptr;
+        bool good = ok_(cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal), "batch graph");
+        if (good) {
+            enqueue_iteration(b, cfl, tol, cap);
+            good = ok_(cudaStreamEndCapture(cap, &graph), "batch graph") &&
+                   ok_(cudaGraphInstantiate(&exec, graph, 0), "batch graph");
+        }
+        if (graph) cudaGraphDestroy(graph);
+        return good;
+    };
+    ok = ok && build_items(b) && capture();
+    int64_t done = 0;
+    int active = b->n_inst;
+    while (ok && done < max_iter) {
+        const int64_t chunk = std::min<int64_t>(check_every, max_iter - done);
+        const int per_iter = 2 + (b->n_cell_items ? 2 : 0) - (b->n_ghost_items ? 0 : 1);
+        for (int64_t i = 0; i < chunk && ok; ++i) {
+            ok = ok_(cudaGraphLaunch(exec, s), "batch graph launch");
+            count_launch(per_iter);
+        }
+        done += chunk;
+        if (!ok || !download_inst(b)) { ok = false; break; }
+        int now = 0;
+        for (const InstDev& I : b->h_inst) now += I.status == 0;
+        if (now == 0) break;
+        if (now != active) {             // drop the frozen instances' work
+            active = now;
+            ok = build_items(b) && ok_(cudaStreamSynchronize(s), "batch items") && capture();
+        }
+    }
+    if (exec) cudaGraphExecDestroy(exec);
+    if (cap) cudaStreamDestroy(cap);
+    return ok ? done : -1;
+}
+
+void reset_counters(Batch* b, int64_t max_iter, bool with_hist) {
+    for (InstDev& I : b->h_inst) {
+        I.status = 0;
+        I.iters = 0;
+        I.max_iter = (int)std::min<int64_t>(max_iter, 1 << 30);
+        I.res0 = 0.0;
+        I.ratio = 1.0;
+        if (!with_hist) I.hist = nullptr;
+    }
+}
+
+}  // namespace
+}  // namespace gb
+
+using namespace gb;
+
+extern "C" {
+
+gbBatch* gbBatchCreate(int n_meshes, cuMesh* const* meshes, int n_instances, const gbBatchInstance* instances) {
+    clear_error();
+    if (n_meshes <= 0 || !meshes || n_instances <= 0 || !instances) {
+        set_error("gbBatchCreate: bad arguments");
+        return nullptr;
+    }
+    Batch* b = new Batch();
+    cudaStream_t s = (cudaStream_t)gbGetStream();
+    b->meshes.assign(meshes, meshes + n_meshes);
+    b->acc.resize(n_meshes);
+    std::vector<MeshTab> tabs(n_meshes);
+    bool ok = true;
+    for (int m = 0; m < n_meshes && ok; ++m) {
+        ok = mesh_access(meshes[m], &b->acc[m]);
+        if (!ok) break;
+        const MeshAccess& A = b->acc[m];
+        if (A.n_regions > kMaxRegions) { set_error("gbBatchCreate: more than 16 regions"); ok = false; break; }
+        std::vector<uint8_t> reg((size_t)A.G, 0);
+        for (int r = 0; r < A.n_regions; ++r)
+            for (uint32_t g = A.region_start[r]; g < A.region_start[r + 1]; ++g) reg[g - A.N] = (uint8_t)r;
+        uint8_t* d = nullptr;
+        ok = balloc(b, d, reg.size(), "batch regions") &&
+             ok_(cudaMemcpyAsync(d, reg.data(), reg.size(), cudaMemcpyHostToDevice, s), "batch regions");
+        const DevMesh& D = *A.dev;
+        tabs[m] = MeshTab{MeshDev{D.cell_geo, D.face_geo, D.start, D.nb, D.lsq, (uint32_t)D.N}, D.ghost, d,
+                          (uint32_t)D.G};
+        b->signature += std::to_string(A.N) + "/";
+    }
+    ok = ok && balloc(b, b->d_mesh, n_meshes, "batch meshes") &&
+         ok_(cudaMemcpyAsync(b->d_mesh, tabs.data(), tabs.size() * sizeof(MeshTab), cudaMemcpyHostToDevice, s),
+             "batch meshes");
+    b->n_inst = n_instances;
+    b->h_inst.assign(n_instances, InstDev{});
+    std::vector<int> per_mesh(n_meshes, 0);
+    for (int i = 0; i < n_instances && ok; ++i) {
+        const gbBatchInstance& src = instances[i];
+        if (src.mesh < 0 || src.mesh >= n_meshes || src.n_bc < 0 || (src.n_bc && !src.bcs)) {
+            set_error("gbBatchCreate: bad instance " + std::to_string(i));
+            ok = false;
+            break;
+        }
+        per_mesh[src.mesh]++;
+        InstDev& I = b->h_inst[i];
+        I.mesh = src.mesh;
+        for (int r = 0; r < kMaxRegions; ++r) I.bc[r] = -1;
+        const MeshAccess& A = b->acc[src.mesh];
+        for (int k = 0; k < src.n_bc; ++k) {
+            const gbBc& c = src.bcs[k];
+            if ((int)c.region_id >= A.n_regions || (c.type != 0 && c.type != 1)) {
+                set_error("gbBatchCreate: bad boundary condition of instance " + std::to_string(i));
+                ok = false;
+                break;
+            }
+            I.bc[c.region_id] = (int)b->h_bcs.size();
+            b->h_bcs.push_back(BcDev{c.type, make_float3(c.mach.x, c.mach.y, c.mach.z), c.pressure, c.temperature});
+        }
+        const int64_t NG = A.N + A.G;
+        for (int k = 0; k < 2 && ok; ++k)
+            ok = balloc(b, I.rho[k], NG, "batch state") && balloc(b, I.rhou[k], NG, "batch state") &&
+                 balloc(b, I.rhoe[k], NG, "batch state");
+        ok = ok && balloc(b, I.g_rho, A.N, "batch gradients") && balloc(b, I.g_rhou, 3 * A.N, "batch gradients") &&
+             balloc(b, I.g_rhoe, A.N, "batch gradients");
+    }
+    for (int m = 0; m < n_meshes; ++m) b->signature += std::to_string(per_mesh[m]) + ",";
+    ok = ok && balloc(b, b->d_bcs, b->h_bcs.size(), "batch bcs") &&
+         ok_(cudaMemcpyAsync(b->d_bcs, b->h_bcs.data(), b->h_bcs.size() * sizeof(BcDev), cudaMemcpyHostToDevice, s),
+             "batch bcs") &&
+         balloc(b, b->d_inst, n_instances, "batch table") && size_partials(b) && build_items(b) && upload_inst(b) &&
+         ok_(cudaStreamSynchronize(s), "gbBatchCreate");
+    if (!ok) {
+        gbBatchFree(b);
+        return nullptr;
+    }
+    return b;
+}
+
+void gbBatchFree(gbBatch* b) {
+    if (!b) return;
+    for (void* p : b->allocations) cudaFree(p);
+    if (b->d_cell_items) cudaFree(b->d_cell_items);
+    if (b->d_ghost_items) cudaFree(b->d_ghost_items);
+    delete b;
+}
+
+int gbBatchInitUniform(gbBatch* b, int inst, gb_vector mach, gb_scalar pressure, gb_scalar temperature) {
+    clear_error();
+    if (!b || inst < 0 || inst >= b->n_inst) { set_error("gbBatchInitUniform: bad instance"); return 1; }
+    const InstDev& I = b->h_inst[inst];
+    const MeshAccess& A = b->acc[I.mesh];
+    // euler_init, src/models/euler.cu:401-404
+    const float r = pressure / temperature;
+    const float c = sqrtf(1.4f * pressure / r);
+    const float3 vel = make_float3(mach.x * c, mach.y * c, mach.z * c);
+    const float e = pressure / 0.4f + 0.5f * r * (vel.x * vel.x + vel.y * vel.y + vel.z * vel.z);
+    for (int k = 0; k < 2; ++k)
+        launch_init(A.N + A.G, I.rho[k], I.rhou[k], I.rhoe[k], r, make_float3(vel.x * r, vel.y * r, vel.z * r), e,
+                    (cudaStream_t)gbGetStream());
+    return ok_(cudaGetLastError(), "gbBatchInitUniform") ? 0 : 1;
+}
+
+int gbBatchSetState(gbBatch* b, int inst, const float* rho, const float* rhou, const float* rhoe) {
+    clear_error();
+    if (!b || inst < 0 || inst >= b->n_inst || !rho || !rhou || !rhoe) { set_error("gbBatchSetState: bad arguments"); return 1; }
+    const InstDev& I = b->h_inst[inst];
+    const MeshAccess& A = b->acc[I.mesh];
+    const int64_t NG = A.N + A.G;
+    cudaStream_t s = (cudaStream_t)gbGetStream();
+    float* stage = nullptr;
+    if (!ok_(cudaMalloc((void**)&stage, NG * 5 * sizeof(float)), "gbBatchSetState")) return 1;
+    bool ok = ok_(cudaMemcpyAsync(stage, rho, NG * 4, cudaMemcpyHostToDevice, s), "gbBatchSetState") &&
+              ok_(cudaMemcpyAsync(stage + NG, rhou, NG * 12, cudaMemcpyHostToDevice, s), "gbBatchSetState") &&
+              ok_(cudaMemcpyAsync(stage + 4 * NG, rhoe, NG * 4, cudaMemcpyHostToDevice, s), "gbBatchSetState");
+    for (int k = 0; k < 2 && ok; ++k) {
+        launch_scatter_scalar(NG, stage, A.d_cell_new, I.rho[k], s);
+        launch_scatter_vector(NG, stage + NG, A.d_cell_new, I.rhou[k], s);
+        launch_scatter_scalar(NG, stage + 4 * NG, A.d_cell_new, I.rhoe[k], s);
+    }
+    ok = ok && ok_(cudaStreamSynchronize(s), "gbBatchSetState");
+    cudaFree(stage);
+    return ok ? 0 : 1;
+}
+
+int gbBatchGetState(gbBatch* b, int inst, float* rho, float* rhou, float* rhoe) {
+    clear_error();
+    if (!b || inst < 0 || inst >= b->n_inst || !rho || !rhou || !rhoe) { set_error("gbBatchGetState: bad arguments"); return 1; }
+    if (!download_inst(b)) return 1;
+    const InstDev& I = b->h_inst[inst];
+    const MeshAccess& A = b->acc[I.mesh];
+    const int64_t NG = A.N + A.G;
+    cudaStream_t s = (cudaStream_t)gbGetStream();
+    float* stage = nullptr;
+    if (!ok_(cudaMalloc((void**)&stage, NG * 5 * sizeof(float)), "gbBatchGetState")) return 1;
+    const int cur = I.cur;
+    launch_gather_scalar(NG, I.rho[cur], A.d_cell_new, stage, s);
+    launch_gather_vector(NG, I.rhou[cur], A.d_cell_new, stage + NG, s);
+    launch_gather_scalar(NG, I.rhoe[cur], A.d_cell_new, stage + 4 * NG, s);
+    bool ok = ok_(cudaMemcpyAsync(rho, stage, NG * 4, cudaMemcpyDeviceToHost, s), "gbBatchGetState") &&
+              ok_(cudaMemcpyAsync(rhou, stage + NG, NG * 12, cudaMemcpyDeviceToHost, s), "gbBatchGetState") &&
+              ok_(cudaMemcpyAsync(rhoe, stage + 4 * NG, NG * 4, cudaMemcpyDeviceToHost, s), "gbBatchGetState") &&
+              ok_(cudaStreamSynchronize(s), "gbBatchGetState");
+    cudaFree(stage);
+    return ok ? 0 : 1;
+}
+
+int gbBatchSetTuning(gbBatch* b, int tile_cells, int schedule) {
+    clear_error();
+    if (!b || tile_cells < kBlock || tile_cells % kBlock || schedule < 0 || schedule > 3) {
+        set_error("gbBatchSetTuning: tile must be a positive multiple of 256, schedule 0..3");
+        return 1;
+    }
+    b->tile = tile_cells;
+    b->schedule = schedule & 1;
+    b->variant = schedule >> 1;
+    return (size_partials(b) && build_items(b) && upload_inst(b)) ? 0 : 1;
+}
+
+int gbBatchGetTuning(gbBatch* b, int* tile_cells, int* schedule) {
+    if (!b) return 1;
+    if (tile_cells) *tile_cells = b->tile;
+    if (schedule) *schedule = b->schedule + 2 * b->variant;
+    return 0;
+}
+
+int gbBatchAutotune(gbBatch* b, gb_scalar cfl, int trial_iters, int* tile_out, int* schedule_out) {
+    clear_error();
+    if (!b || trial_iters <= 0) { set_error("gbBatchAutotune: bad arguments"); return 1; }
+    auto hit = g_tuning_cache.find(b->signature);
+    if (hit == g_tuning_cache.end()) {
+        cudaStream_t s = (cudaStream_t)gbGetStream();
+        // save every instance's state; trials run from it and it is restored
+        std::vector<std::vector<void*>> saved(b->n_inst);
+        bool ok = download_inst(b);
+        for (int i = 0; i < b->n_inst && ok; ++i) {
+            const InstDev& I = b->h_inst[i];
+            const MeshAccess& A = b->acc[I.mesh];
+            const int64_t NG = A.N + A.G;
+            const size_t bytes[3] = {(size_t)NG * 4, (size_t)NG * 16, (size_t)NG * 4};
+            const void* src[3] = {I.rho[I.cur], I.rhou[I.cur], I.rhoe[I.cur]};
+            for (int k = 0; k < 3 && ok; ++k) {
+                void* p = nullptr;
+                ok = ok_(cudaMalloc(&p, bytes[k]), "gbBatchAutotune") &&
+                     ok_(cudaMemcpyAsync(p, src[k], bytes[k], cudaMemcpyDeviceToDevice, s), "gbBatchAutotune");
+                saved[i].push_back(p);
+            }
+        }
+        const std::vector<InstDev> base = b->h_inst;
+        cudaEvent_t e0, e1;
+        cudaEventCreate(&e0);
+        cudaEventCreate(&e1);
+        float best = 1e30f;
+        Tuning best_t{b->tile, b->schedule, b->variant};
+        const int tiles[] = {256, 512, 1024, 2048};
+        for (int var = 0; var < 2 && ok; ++var)
+        for (int sched = 0; sched < 2 && ok; ++sched) {
+            for (int tile : tiles) {
+                if (!ok) break;
+                b->h_inst = base;
+                b->tile = tile;
+                b->schedule = sched;
+                b->variant = var;
+                reset_counters(b, 1 << 30, false);
+                ok = size_partials(b) && build_items(b) && upload_inst(b);
+                // one untimed iteration, then the timed trial
+                if (ok) enqueue_iteration(b, cfl, 0.0, s);
+                cudaEventRecord(e0, s);
+                for (int it = 0; it < trial_iters && ok; ++it) enqueue_iteration(b, cfl, 0.0, s);
+                cudaEventRecord(e1, s);
+                ok = ok && ok_(cudaEventSynchronize(e1), "gbBatchAutotune");
+                float ms = 0.f;
+                cudaEventElapsedTime(&ms, e0, e1);
+                if (ok && ms < best) { best = ms; best_t = Tuning{tile, sched, var}; }
+                // restore the states
+                for (int i = 0; i < b->n_inst && ok; ++i) {
+                    const InstDev& I = base[i];
+                    const MeshAccess& A = b->acc[I.mesh];
+                    const int64_t NG = A.N + A.G;
+                    for (int k = 0; k < 2 && ok; ++k)
+                        ok = ok_(cudaMemcpyAsync(I.rho[k], saved[i][0], NG * 4, cudaMemcpyDeviceToDevice, s), "restore") &&
+                             ok_(cudaMemcpyAsync(I.rhou[k], saved[i][1], NG * 16, cudaMemcpyDeviceToDevice, s), "restore") &&
+                             ok_(cudaMemcpyAsync(I.rhoe[k], saved[i][2], NG * 4, cudaMemcpyDeviceToDevice, s), "restore");
+                }
+            }
+        }
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        cudaStreamSynchronize(s);
+        for (auto& v : saved)
+            for (void* p : v) cudaFree(p);
+        b->h_inst = base;
+        for (InstDev& I : b->h_inst) I.cur = 0;   // the saved states were put in both buffers
+        if (!ok) return 1;
+        g_tuning_cache[b->signature] = best_t;
+        hit = g_tuning_cache.find(b->signature);
+    }
+    b->tile = hit->second.tile;
+    b->schedule = hit->second.schedule;
+    b->variant = hit->second.variant;
+    if (!(size_partials(b) && build_items(b) && upload_inst(b))) return 1;
+    if (tile_out) *tile_out = b->tile;
+    if (schedule_out) *schedule_out = b->schedule + 2 * b->variant;
+    return 0;
+}
+
+int64_t gbBatchRun(gbBatch* b, gb_scalar cfl, int64_t max_iter, double tolerance, int check_every,
+                   int64_t* iterations, double* ratios, int* status, double* history) {
+    clear_error();
+    if (!b || max_iter < 0) { set_error("gbBatchRun: bad arguments"); return -1; }
+    if (check_every <= 0) check_every = 100;
+    if (!download_inst(b)) return -1;
+    double* d_hist = nullptr;
+    if (history && max_iter > 0) {
+        if (!ok_(cudaMalloc((void**)&d_hist, (size_t)b->n_inst * max_iter * sizeof(double)), "gbBatchRun") ||
+            !ok_(cudaMemsetAsync(d_hist, 0, (size_t)b->n_inst * max_iter * sizeof(double), (cudaStream_t)gbGetStream()),
+                 "gbBatchRun"))
+            return -1;
+        for (int i = 0; i < b->n_inst; ++i) b->h_inst[i].hist = d_hist + (size_t)i * max_iter;
+    }
+    reset_counters(b, max_iter, history != nullptr);
+    if (!upload_inst(b)) { if (d_hist) cudaFree(d_hist); return -1; }
+    const int64_t done = max_iter > 0 ? run_loop(b, cfl, max_iter, tolerance, check_every) : 0;
+    bool ok = done >= 0 && download_inst(b);
+    if (ok && history) {
+        ok = ok_(cudaMemcpy(history, d_hist, (size_t)b->n_inst * max_iter * sizeof(double), cudaMemcpyDeviceToHost),
+                 "gbBatchRun");
+    }
+    if (d_hist) {
+        cudaFree(d_hist);
+        for (InstDev& I : b->h_inst) I.hist = nullptr;
+        upload_inst(b);
+    }
+    if (!ok) return -1;
+    for (int i = 0; i < b->n_inst; ++i) {
+        if (iterations) iterations[i] = b->h_inst[i].iters;
+        if (ratios) ratios[i] = b->h_inst[i].ratio;
+        if (status) status[i] = b->h_inst[i].status;
+    }
+    return done;
+}
+
+}  // extern "C"

@@ -19,6 +19,8 @@
 
 #include <cstdint>
 
+#include "graphite_b200.h"
+
 namespace gb {
 
 struct DevMesh {
@@ -88,5 +90,16 @@ void launch_scatter_scalar(int64_t n, const float* src, const uint32_t* idx, flo
 void launch_scatter_vector(int64_t n, const float* src3, const uint32_t* idx, float4* dst, cudaStream_t s);
 
 void count_launch(int n = 1);
+
+// Device view of a loaded mesh, for other translation units of the library.
+struct MeshAccess {
+    const DevMesh* dev;
+    const uint32_t* d_cell_new;            // reference order -> device order, N + G
+    const uint32_t* region_start;          // device ghost ranges per region (host array)
+    int n_regions;
+    int64_t N, G;
+};
+bool mesh_access(::cuMesh* mesh, MeshAccess* out);
+bool reference_momentum();
 
 }  // namespace gb

@@ -360,13 +360,13 @@ def _ogrid_lines(cx, cz, fx, fz, d, delta):
 
 
 def airfoil_2d_prisms(n_around: int, n_radial: int, span: float = 0.1, r_far: float = 20.0,
-                      first: float = 2e-3) -> ElementMesh:
+                      first: float = 2e-3, cluster: float = 0.5) -> ElementMesh:
     """2-D NACA 0012 O-grid, quads cut into 2 triangles, extruded one layer in y.
 
     Triangles = 2 * n_around * n_radial = cells (prisms).  Regions: wing,
     farfield, sides (the two span planes).
     """
-    xc, zc = naca0012_contour(n_around)
+    xc, zc = naca0012_contour(n_around, cluster=cluster)
     centre = np.array([0.5, 0.0])
     theta = 2.0 * math.pi * np.arange(n_around) / n_around     # even far-field angles
     d = _radial(n_radial, first / r_far, 1.0)

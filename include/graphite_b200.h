@@ -250,6 +250,56 @@ int64_t gbEulerRun(cuMesh* mesh, FvmField* rho, FvmField* rhou, FvmField* rhoe, 
 /* Launches of this library's kernels since load (for accounting). */
 uint64_t gbKernelLaunchCount(void);
 
+/* ------------------------------------------------ batched instances --- */
+
+/* Many instances (mesh, boundary conditions) advanced together: each
+ * iteration is four persistent kernels over all active instances (ghosts,
+ * gradients + limiters, flux + update, per-instance residual and
+ * convergence), replayed as a CUDA graph.  An instance stops updating (is
+ * frozen) when its residual ratio drops below the tolerance.  Each instance
+ * computes exactly what a plain solve of it computes.  No counterpart in the
+ * reference. */
+typedef struct gbBatchImpl gbBatch;
+
+typedef struct gbBatchInstance {
+    int mesh;            /* index into the meshes passed to gbBatchCreate */
+    int n_bc;
+    const gbBc* bcs;     /* as for gbEulerRun (region ids of that mesh) */
+} gbBatchInstance;
+
+gbBatch* gbBatchCreate(int n_meshes, cuMesh* const* meshes, int n_instances, const gbBatchInstance* instances);
+void gbBatchFree(gbBatch* batch);
+
+/* Uniform free-stream state (euler_init) for one instance. */
+int gbBatchInitUniform(gbBatch* batch, int instance, gb_vector mach, gb_scalar pressure, gb_scalar temperature);
+
+/* Instance state from / to host arrays in the reference's layout and cell
+ * order: rho[n], rhou[3n], rhoe[n] with n = cells + ghosts of its mesh. */
+int gbBatchSetState(gbBatch* batch, int instance, const float* rho, const float* rhou, const float* rhoe);
+int gbBatchGetState(gbBatch* batch, int instance, float* rho, float* rhou, float* rhoe);
+
+/* Work decomposition: cells per work item (multiple of 256) and schedule =
+ * order + 2 * register variant; order 0 runs instance by instance, 1 tile by
+ * tile across the instances of a mesh; variant 0 / 1 compiles the gradient
+ * and flux kernels for 3 / 4 and 2 / 3 resident blocks per SM. */
+int gbBatchSetTuning(gbBatch* batch, int tile_cells, int schedule);
+int gbBatchGetTuning(gbBatch* batch, int* tile_cells, int* schedule);
+
+/* Times trial_iters iterations of every (tile, schedule) candidate from the
+ * current states (restored afterwards) and keeps the fastest; results are
+ * cached per (mesh sizes, instances per mesh) for the process. */
+int gbBatchAutotune(gbBatch* batch, gb_scalar cfl, int trial_iters, int* tile_cells, int* schedule);
+
+/* Runs until every instance has converged (residual / first residual <
+ * tolerance), hit max_iter, or produced a non-finite residual; polls every
+ * check_every iterations.  Per-instance outputs (arrays of n_instances, may
+ * be NULL): iterations, final residual ratio, status (1 converged, 2
+ * iteration cap, 3 not finite); history (n_instances x max_iter doubles, may
+ * be NULL) receives the residual sums.  Returns the iterations of the loop,
+ * or -1 on error. */
+int64_t gbBatchRun(gbBatch* batch, gb_scalar cfl, int64_t max_iter, double tolerance, int check_every,
+                   int64_t* iterations, double* ratios, int* status, double* history);
+
 /* Sum of n float values in device memory into *result (one double in device
  * memory), accumulated in float64 in a fixed order: the reduction behind
  * FvmFieldReduceSum, for callers that cannot allocate device memory -- code
