@@ -55,6 +55,18 @@ class EulerBatch:
         capi.check(self.lib.gbBatchGetState(self.h, i, r.ctypes.data, u.ctypes.data, e.ctypes.data), "gbBatchGetState")
         return r, u.reshape(n, 3), e
 
+    def set_residual_scale(self, i: int, res0: float) -> None:
+        """Divide instance i's residuals by res0 instead of its first residual (0: default)."""
+        capi.check(self.lib.gbBatchSetResidualScale(self.h, i, float(res0)), "gbBatchSetResidualScale")
+
+    def wall_force(self, i: int, region: str) -> np.ndarray:
+        """Pressure force on a boundary region of instance i (gbBatchWallForce), float64 [3]."""
+        c = self.cases[self.instance_case[i]]
+        rid = self.lib.cuMeshGetRegionId(c.mesh, region.encode())
+        f = np.zeros(3, np.float64)
+        capi.check(self.lib.gbBatchWallForce(self.h, i, rid, f.ctypes.data), "gbBatchWallForce")
+        return f
+
     def set_tuning(self, tile: int, schedule: int) -> None:
         capi.check(self.lib.gbBatchSetTuning(self.h, tile, schedule), "gbBatchSetTuning")
 

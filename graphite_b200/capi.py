@@ -103,6 +103,27 @@ _PROTOS = {
     "gbKernelLaunchCount": (C.c_uint64, []),
     "gbReduceSumNoAlloc": (C.c_int, [C.c_void_p, C.c_uint64, C.c_void_p, C.c_void_p]),
     "gbBatchCreate": (C.c_void_p, [C.c_int, C.POINTER(MeshP), C.c_int, C.POINTER(gbBatchInstance)]),
+    "gbBatchSetResidualScale": (C.c_int, [C.c_void_p, C.c_int, C.c_double]),
+    "gbWallForce": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint, C.c_void_p]),
+    "gbBatchWallForce": (C.c_int, [C.c_void_p, C.c_int, C.c_uint, C.c_void_p]),
+    "gbWarmStartCreate": (C.c_void_p, [C.c_void_p, C.c_uint, C.c_uint64]),
+    "gbWarmStartFree": (None, [C.c_void_p]),
+    "gbWarmStartParamCount": (C.c_int64, []),
+    "gbWarmStartGetWeights": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "gbWarmStartSetWeights": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "gbWarmStartGetScales": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    "gbWarmStartSetScales": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "gbWarmStartGetFeatures": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "gbWarmStartAddBatchField": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, gb_vector, C.c_float, C.c_float]),
+    "gbWarmStartAddField": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, gb_vector, C.c_float,
+                                      C.c_float]),
+    "gbWarmStartFieldCount": (C.c_int64, [C.c_void_p]),
+    "gbWarmStartTrain": (C.c_int64, [C.c_void_p, C.c_int, C.c_int, C.c_float, C.c_void_p, C.c_int64]),
+    "gbWarmStartPredictBatch": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, gb_vector, C.c_float, C.c_float]),
+    "gbWarmStartPredict": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, gb_vector, C.c_float,
+                                     C.c_float]),
+    "gbWarmStartGradient": (C.c_int, [C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "gbWarmStartForward": (C.c_int, [C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p]),
     "gbBatchFree": (None, [C.c_void_p]),
     "gbBatchInitUniform": (C.c_int, [C.c_void_p, C.c_int, gb_vector, C.c_float, C.c_float]),
     "gbBatchSetState": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]),

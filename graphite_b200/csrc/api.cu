@@ -397,6 +397,23 @@ bool mesh_access(cuMesh* mesh, MeshAccess* out) {
     out->n_regions = (int)mi->topo.regions.size();
     out->N = mi->topo.N;
     out->G = mi->topo.G;
+    out->topo = &mi->topo;
+    out->num = &mi->num;
+    return true;
+}
+
+bool field_access(FvmField* f, cuMesh* mesh, int comps, FieldAccess* out) {
+    FieldImpl* fi = impl(f);
+    if (!fi || !fi->val[0]) { set_error("null or unallocated field"); return false; }
+    if (mesh ? !bind(mesh, f, comps, "field") : fi->comps != comps) {
+        if (!mesh) set_error("field has the wrong number of components");
+        return false;
+    }
+    out->val[0] = fi->val[0];
+    out->val[1] = fi->val[1];
+    out->cur = fi->cur;
+    out->comps = fi->comps;
+    out->size = fi->size;
     return true;
 }
 

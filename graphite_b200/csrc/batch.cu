@@ -45,6 +45,7 @@ struct InstDev {
     int iters;
     int max_iter;
     double res0;
+    double res0_fixed;    // > 0: residuals are divided by this instead of the first one
     double ratio;
     int bc[kMaxRegions];  // boundary condition per region (index into the BC table), -1 none
 };
@@ -140,7 +141,7 @@ __global__ void k_batch_reduce(InstDev* insts, double tol) {
     for (int k = threadIdx.x; k < I.n_tiles; k += blockDim.x) s += I.partials[k];
     const double bs = block_sum(s);
     if (threadIdx.x == 0) {
-        if (I.iters == 0) I.res0 = bs;
+        if (I.iters == 0) I.res0 = I.res0_fixed > 0.0 ? I.res0_fixed : bs;
         const double ratio = I.res0 > 0.0 ? bs / I.res0 : 0.0;
         if (I.hist) I.hist[I.iters] = bs;
         I.iters += 1;
@@ -648,4 +649,28 @@ int64_t gbBatchRun(gbBatch* b, gb_scalar cfl, int64_t max_iter, double tolerance
     return done;
 }
 
+int gbBatchSetResidualScale(gbBatch* b, int inst, double res0) {
+    clear_error();
+    if (!b || inst < 0 || inst >= b->n_inst || !(res0 >= 0.0)) { set_error("gbBatchSetResidualScale: bad arguments"); return 1; }
+    if (!download_inst(b)) return 1;
+    b->h_inst[inst].res0_fixed = res0;
+    return upload_inst(b) && ok_(cudaStreamSynchronize((cudaStream_t)gbGetStream()), "gbBatchSetResidualScale") ? 0 : 1;
+}
+
 }  // extern "C"
+
+namespace gb {
+bool batch_instance(gbBatch* b, int inst, BatchInstanceAccess* out) {
+    if (!b || inst < 0 || inst >= b->n_inst) { set_error("bad batch instance"); return false; }
+    if (!download_inst(b)) return false;
+    const InstDev& I = b->h_inst[inst];
+    for (int k = 0; k < 2; ++k) {
+        out->rho[k] = I.rho[k];
+        out->rhou[k] = I.rhou[k];
+        out->rhoe[k] = I.rhoe[k];
+    }
+    out->cur = I.cur;
+    out->mesh = b->meshes[I.mesh];
+    return true;
+}
+}  // namespace gb

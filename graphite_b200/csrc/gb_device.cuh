@@ -91,6 +91,9 @@ void launch_scatter_vector(int64_t n, const float* src3, const uint32_t* idx, fl
 
 void count_launch(int n = 1);
 
+struct Topology;
+struct Numbering;
+
 // Device view of a loaded mesh, for other translation units of the library.
 struct MeshAccess {
     const DevMesh* dev;
@@ -98,8 +101,31 @@ struct MeshAccess {
     const uint32_t* region_start;          // device ghost ranges per region (host array)
     int n_regions;
     int64_t N, G;
+    const Topology* topo;                  // host topology (reference numbering)
+    const Numbering* num;                  // reference <-> device numbering
 };
 bool mesh_access(::cuMesh* mesh, MeshAccess* out);
 bool reference_momentum();
+
+// Device buffers of a field (device cell order; val[cur] is the current value).
+struct FieldAccess {
+    void* val[2];
+    int cur;
+    int comps;                             // 1 scalar (float), 3 vector (float4)
+    size_t size;
+};
+// Binds the field to `mesh` (its device order becomes the mesh's) and checks
+// its size and number of components.
+bool field_access(::FvmField* f, ::cuMesh* mesh, int comps, FieldAccess* out);
+
+// State buffers of one instance of a batch (device cell order of its mesh).
+struct BatchInstanceAccess {
+    float* rho[2];
+    float4* rhou[2];
+    float* rhoe[2];
+    int cur;
+    ::cuMesh* mesh;
+};
+bool batch_instance(::gbBatch* b, int inst, BatchInstanceAccess* out);
 
 }  // namespace gb

@@ -144,6 +144,13 @@ class EulerCase:
         self.lib.VarGpuToCpu(self.error)
         return capi.field_values(self.error)
 
+    def wall_force(self, region: str) -> np.ndarray:
+        """Pressure force on a boundary region (gbWallForce), float64 [3]."""
+        rid = self.lib.cuMeshGetRegionId(self.mesh, region.encode())
+        f = np.zeros(3, np.float64)
+        capi.check(self.lib.gbWallForce(self.mesh, self.rho, self.rhou, self.rhoe, rid, f.ctypes.data), "gbWallForce")
+        return f
+
     def close(self) -> None:
         if getattr(self, "mesh", None):
             for f in (self.rho, self.rhou, self.rhoe, self.error):

@@ -300,6 +300,71 @@ int gbBatchAutotune(gbBatch* batch, gb_scalar cfl, int trial_iters, int* tile_ce
 int64_t gbBatchRun(gbBatch* batch, gb_scalar cfl, int64_t max_iter, double tolerance, int check_every,
                    int64_t* iterations, double* ratios, int* status, double* history);
 
+/* Divide instance `instance`'s residuals by res0 instead of by its first
+ * residual (0 restores the default).  A warm-started instance given the first
+ * residual of its cold start converges to the same absolute level as the cold
+ * start does.  No counterpart in the reference. */
+int gbBatchSetResidualScale(gbBatch* batch, int instance, double res0);
+
+/* ---- Learned warm start (no counterpart in the reference) ----
+ * A per-cell MLP (inputs: centroid x, y, z, wall distance, Mach, sin AoA,
+ * cos AoA, 1; three SiLU layers of 128; outputs rho, rho u, rho v, rho w,
+ * rho E) trained on converged fields of one mesh and used to predict the
+ * initial state of new cases.  The angle of attack is taken in the x-z plane
+ * (mach = M (cos a, 0, sin a)).  Weights are 36864 floats in the order
+ * W1[128][16] (inputs 8..15 are zero padding), W2[128][128], W3[128][128],
+ * W4[16][128] (outputs 5..15 are padding); layer k computes
+ * z = W_k a_{k-1}. */
+typedef struct gbWarmStartImpl gbWarmStart;
+
+/* mesh may be NULL (then only gbWarmStartGradient / gbWarmStartForward and
+ * the weight calls work); wall_region = cuMeshGetRegionId of the wall. */
+gbWarmStart* gbWarmStartCreate(cuMesh* mesh, unsigned wall_region, uint64_t seed);
+void gbWarmStartFree(gbWarmStart* ws);
+int64_t gbWarmStartParamCount(void);
+int gbWarmStartGetWeights(gbWarmStart* ws, float* weights);
+int gbWarmStartSetWeights(gbWarmStart* ws, const float* weights);
+/* geometry[4] = wall centre xyz and extent L of the input map
+ * u -> u / sqrt(1 + u^2), u = offset / L; target[5] = output scales s
+ * (prediction = free stream + s * output). */
+int gbWarmStartGetScales(gbWarmStart* ws, float* geometry, float* target);
+int gbWarmStartSetScales(gbWarmStart* ws, const float* target);
+/* Mapped geometry inputs (x', y', z', wall distance') per interior cell,
+ * reference cell order: geo[4 n]. */
+int gbWarmStartGetFeatures(gbWarmStart* ws, float* geo);
+/* Adds a converged field as training data: the current state of a batch
+ * instance on the same mesh, or three fields. */
+int gbWarmStartAddBatchField(gbWarmStart* ws, gbBatch* batch, int instance, gb_vector mach, gb_scalar pressure,
+                             gb_scalar temperature);
+int gbWarmStartAddField(gbWarmStart* ws, FvmField* rho, FvmField* rhou, FvmField* rhoe, gb_vector mach,
+                        gb_scalar pressure, gb_scalar temperature);
+int64_t gbWarmStartFieldCount(gbWarmStart* ws);
+/* Adam (beta 0.9 / 0.999, eps 1e-8) on the mean squared error of the scaled
+ * outputs; each step takes tiles_per_cta tiles of 128 cells per SM, tiles
+ * shuffled per epoch.  loss_history (may be NULL) receives up to history_len
+ * per-step losses.  Returns the number of steps, or -1. */
+int64_t gbWarmStartTrain(gbWarmStart* ws, int epochs, int tiles_per_cta, float lr, double* loss_history,
+                         int64_t history_len);
+/* Writes the predicted state into a batch instance / three fields (both
+ * value buffers of interior cells; ghosts are set by the next iteration's
+ * boundary conditions). */
+int gbWarmStartPredictBatch(gbWarmStart* ws, gbBatch* batch, int instance, gb_vector mach, gb_scalar pressure,
+                            gb_scalar temperature);
+int gbWarmStartPredict(gbWarmStart* ws, FvmField* rho, FvmField* rhou, FvmField* rhoe, gb_vector mach,
+                       gb_scalar pressure, gb_scalar temperature);
+/* Explicit samples, for checking the kernels: x[n][8] inputs, t[n][5] scaled
+ * targets.  Gradient: grad[36864] of the loss mean((y - t)^2) and the loss;
+ * forward: y[n][5]. */
+int gbWarmStartGradient(gbWarmStart* ws, int64_t n, const float* x, const float* t, float* grad, double* loss);
+int gbWarmStartForward(gbWarmStart* ws, int64_t n, const float* x, float* y);
+
+/* Pressure force on boundary region region_id (sum of p A n over its faces,
+ * n pointing out of the fluid, p of the adjacent interior cell), float64,
+ * deterministic; force[3].  Lift and drag are its components normal and
+ * parallel to the free stream.  No counterpart in the reference. */
+int gbWallForce(cuMesh* mesh, FvmField* rho, FvmField* rhou, FvmField* rhoe, unsigned region_id, double* force);
+int gbBatchWallForce(gbBatch* batch, int instance, unsigned region_id, double* force);
+
 /* Sum of n float values in device memory into *result (one double in device
  * memory), accumulated in float64 in a fixed order: the reduction behind
  * FvmFieldReduceSum, for callers that cannot allocate device memory -- code

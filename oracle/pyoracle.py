@@ -208,3 +208,37 @@ def set_threads(n: int) -> None:
 
 def max_threads() -> int:
     return int(load().orc_max_threads())
+
+
+def wall_force(mesh: "OracleMesh", rho, rhou, rhoe, region) -> np.ndarray:
+    """Pressure force on a boundary region from a state in reference order,
+    in float64: the sum over the region's ghosts of p A n, with p the pressure
+    of the ghost's interior cell and n its face normal oriented away from that
+    cell (the orientation of src/models/euler.cu:422-434)."""
+    r = mesh.region_id(region) if isinstance(region, str) else int(region)
+    gs, gid = mesh.get("ghost_cell_starts"), mesh.get("ghost_cell_ids")
+    cfs, cf, cc = mesh.get("cell_faces_starts"), mesh.get("cell_faces"), mesh.get("cell_connects")
+    area = mesh.get("face_areas")
+    nrm = mesh.get("face_normals").reshape(-1, 3)
+    fctr = mesh.get("face_centers").reshape(-1, 3)
+    cctr = mesh.get("cell_centers").reshape(-1, 3)
+    g = gid[gs[r]:gs[r + 1]]
+    c1 = cc[cfs[g]]
+    face = cf[cfs[g]]
+    n = nrm[face]
+    sign = np.where(np.einsum("ij,ij->i", n, fctr[face] - cctr[c1]) >= 0, 1.0, -1.0)
+    rho = np.asarray(rho, np.float64)
+    rhou = np.asarray(rhou, np.float64).reshape(-1, 3)
+    rhoe = np.asarray(rhoe, np.float64)
+    p = 0.4 * (rhoe[c1] - 0.5 * np.einsum("ij,ij->i", rhou[c1], rhou[c1]) / rho[c1])
+    return np.sum((p * area[face] * sign)[:, None] * n, axis=0)
+
+
+def lift_drag(force, mach) -> tuple:
+    """(lift, drag): components of the force normal and parallel to the free
+    stream, the normal taken in the x-z plane (mach = M (cos a, 0, sin a))."""
+    m = np.asarray(mach, np.float64)
+    d = m / np.linalg.norm(m)
+    l = np.array([-d[2], 0.0, d[0]])
+    f = np.asarray(force, np.float64)
+    return float(f @ l), float(f @ d)
