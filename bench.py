@@ -304,10 +304,12 @@ def run_ours(args, rank, world, local_rank):
                "min_residual_ratio": float(np.min(ratio)), "max_iterations": args.max_iters,
                "metric": "sum over cells of (F_rho^2+|F_rhou|^2+F_rhoE^2) V, relative to iteration 0"}
 
-    # ---- batched sweep (config 3), optional ----
-    batch = None
-    if rank == 0 and args.batch:
+    # ---- batched sweep (config 3) and learned warm start (config 4), one GPU ----
+    batch = warm = None
+    if rank == 0 and world == 1 and not args.skip_batch:
         batch = run_batch_comparison(args, dev_stream)
+    if rank == 0 and world == 1 and not args.skip_warm:
+        warm = run_warm_start(args, dev_stream)
 
     # ---- CPU baseline (rank 0, N = 1) ----
     cpu = None
@@ -336,6 +338,7 @@ def run_ours(args, rank, world, local_rank):
         "residual_finite": finite,
         "time_to_1e-3": ttr,
         "batched_airfoil_sweep": batch,
+        "batched_warm_start": warm,
         "cpu_baseline": cpu,
     }
     case.close()
@@ -477,6 +480,136 @@ def run_batch_comparison(args, dev_stream):
     }
 
 
+WARM_SEED = 20261204
+WARM_TRAIN, WARM_HELD = 512, 64
+WARM_EPOCHS, WARM_TILES, WARM_LR = 200, 8, 1e-3
+
+
+def run_warm_start(args, dev_stream):
+    """Config 4: the learned warm start on the 120k airfoil mesh.  512 seeded
+    training draws (Mach ~ U[0.3, 0.8], AoA ~ U[-4, 8] deg) are solved cold
+    with the batched solver to a 1e-3 residual drop, the MLP trains on them
+    (200 epochs, Adam 1e-3), and 64 held-out draws are solved three ways:
+    plain cold single-instance solves (gbEulerRun, one after another),
+    batched cold, and batched warm (each instance stops at 1e-3 times the
+    first residual of its cold start).  Wall-clock is host time with the
+    device synchronised on both sides."""
+    import torch
+    from graphite_b200 import meshgen
+    from graphite_b200.batch import EulerBatch
+    from graphite_b200.euler import EulerCase, lift_drag
+    from graphite_b200.warmstart import WarmStart, solve_warm
+
+    cache = os.path.join(tempfile.gettempdir(), "graphite_b200_bench")
+    os.makedirs(cache, exist_ok=True)
+    path = os.path.join(cache, "airfoil_120000.su2")
+    if not os.path.exists(path):
+        tmp = path + f".tmp{os.getpid()}"
+        meshgen.airfoil_extruded(120_000).write_su2(tmp)
+        os.replace(tmp, path)
+    c = EulerCase(path)
+    rng = np.random.default_rng(WARM_SEED)
+    draws = [(float(rng.uniform(0.3, 0.8)), float(rng.uniform(-4.0, 8.0))) for _ in range(WARM_TRAIN + WARM_HELD)]
+    train, held = draws[:WARM_TRAIN], draws[WARM_TRAIN:]
+    tol, cap, cfl = 1e-3, SWEEP_MAX_ITERS, SWEEP_CFL
+
+    def clock():
+        torch.cuda.synchronize()
+        return time.perf_counter()
+
+    # 1. training data: batched cold solves
+    t0 = clock()
+    ws = WarmStart(c, wall="wing", seed=WARM_SEED)
+    with EulerBatch([c], [(0, airfoil_case(m, a)[1]) for m, a in train]) as b:
+        b.autotune(cfl, trial_iters=3)
+        for i, (m, a) in enumerate(train):
+            b.init_uniform(i, airfoil_case(m, a)[0], P_INF, T_INF)
+        _, gen_its, _, gen_st = b.run(cfl, cap, tolerance=tol, check_every=200)
+        for i, (m, a) in enumerate(train):
+            if gen_st[i] == 1:
+                ws.add_batch_field(b, i, airfoil_case(m, a)[0], P_INF, T_INF)
+    t_gen = clock() - t0
+    # 2. training
+    t0 = clock()
+    steps, hist = ws.train(WARM_EPOCHS, tiles_per_cta=WARM_TILES, lr=WARM_LR, history=1 << 22)
+    t_train = clock() - t0
+    samples = WARM_EPOCHS * ws.n_fields * c.n_cells
+    fwd_flop = 2 * (16 * 128 + 2 * 128 * 128 + 128 * 16)       # per sample, padded GEMM shapes
+    # 3. plain cold single-instance solves
+    cases = [(airfoil_case(m, a)[0], P_INF, T_INF) for m, a in held]
+    plain_its, plain_ld, plain_ld_next = [], [], []
+    t_plain = 0.0
+    for (m, a), (mv, p, t) in zip(held, cases):
+        bcs = airfoil_case(m, a)[1]
+        c.init(mv, p, t)
+        t0 = clock()
+        h = c.run(bcs, cfl, cap, tolerance=tol, check_every=100)
+        t_plain += clock() - t0
+        r = h / h[0]
+        plain_its.append(int(np.argmax(r < tol)) + 1 if np.any(r < tol) else len(h))
+        plain_ld.append(lift_drag(c.wall_force("wing"), mv))
+        c.run(bcs, cfl, 1000)                 # how far the plain solve still moves
+        plain_ld_next.append(lift_drag(c.wall_force("wing"), mv))
+    plain_ld, plain_ld_next = np.array(plain_ld), np.array(plain_ld_next)
+    # 4. batched cold / batched warm
+    spec = [(0, airfoil_case(m, a)[1]) for m, a in held]
+    with EulerBatch([c], spec) as b:
+        b.autotune(cfl, trial_iters=3)
+        t0 = clock()
+        cold_its, _, cold_st, _ = solve_warm(b, [None] * len(held), cases, cfl, cap, tol)
+        t_bcold = clock() - t0
+        t0 = clock()
+        warm_its, _, warm_st, fell = solve_warm(b, [ws] * len(held), cases, cfl, cap, tol)
+        t_warm = clock() - t0
+        warm_ld = np.array([lift_drag(b.wall_force(i, "wing"), cases[i][0]) for i in range(len(held))])
+        warm_rho = [b.get_state(i)[0][: c.n_cells] for i in range(len(held))]
+    # plain-solve density at its 1e-3 point, for the field check
+    rho_diff = []
+    for k, ((m, a), (mv, p, t)) in enumerate(zip(held, cases)):
+        if k >= 8:
+            break
+        c.init(mv, p, t)
+        c.run(airfoil_case(m, a)[1], cfl, cap, tolerance=tol, check_every=1)
+        rp = c.fields()[0][: c.n_cells]
+        rho_diff.append(float(np.linalg.norm(warm_rho[k] - rp) / np.linalg.norm(rp)))
+    ws.close()
+    c.close()
+    n = len(held)
+    lmax = float(np.max(np.abs(plain_ld[:, 0])))
+    dl = np.abs(warm_ld[:, 0] - plain_ld[:, 0]) / lmax
+    per_plain, per_warm, per_bcold = t_plain / n, t_warm / n, t_bcold / n
+    saving = per_plain - per_warm
+    return {
+        "mesh": "NACA 0012 airfoil, 120,000 prisms (one layer)", "cells": int(c.n_cells),
+        "train_draws": WARM_TRAIN, "held_out_draws": n, "seed": WARM_SEED, "mach_range": [0.3, 0.8],
+        "aoa_range_deg": [-4.0, 8.0], "cfl": cfl, "tolerance": tol, "max_iterations": cap,
+        "criterion": "residual sum < 1e-3 x the first residual of the case's cold start",
+        "data_generation": {"seconds": t_gen, "fields": int((gen_st == 1).sum()),
+                            "iterations_median": int(np.median(gen_its))},
+        "training": {"seconds": t_train, "epochs": WARM_EPOCHS, "steps": steps, "tiles_per_cta": WARM_TILES,
+                     "lr": WARM_LR, "samples_per_s": samples / t_train,
+                     "tensor_tflops": samples * 3 * fwd_flop / t_train / 1e12,
+                     "loss_first": float(np.mean(hist[:10])), "loss_last": float(np.mean(hist[-100:]))},
+        "plain_cold": {"seconds": t_plain, "seconds_per_case": per_plain, "iterations": plain_its},
+        "batched_cold": {"seconds": t_bcold, "seconds_per_case": per_bcold, "iterations": cold_its.tolist(),
+                         "converged": int((cold_st == 1).sum())},
+        "batched_warm": {"seconds": t_warm, "seconds_per_case": per_warm, "iterations": warm_its.tolist(),
+                         "converged": int((warm_st == 1).sum()), "fell_back_to_free_stream": int(fell.sum())},
+        "speedup_per_case_batched_warm_vs_plain": per_plain / per_warm,
+        "speedup_per_case_batched_cold_vs_plain": per_plain / per_bcold,
+        "break_even_cases_incl_training": (t_gen + t_train) / saving if saving > 0 else None,
+        "vs_plain": {
+            "lift_diff_median": float(np.median(dl)),
+            "lift_diff_max": float(np.max(dl)),
+            "drag_diff_max": float(np.max(np.abs(warm_ld[:, 1] - plain_ld[:, 1])) / lmax),
+            "plain_lift_change_over_next_1000_iterations_median":
+                float(np.median(np.abs(plain_ld_next[:, 0] - plain_ld[:, 0]) / lmax)),
+            "rho_l2_rel_diff_first8": rho_diff,
+            "normalisation": "differences divided by the largest |lift| of the plain solves",
+        },
+    }
+
+
 def run_reference(args, rank, world):
     """The oracle port on the host cores: each step is one bounded sample (a
     block of cells) of the iteration."""
@@ -529,7 +662,8 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--skip-convergence", action="store_true")
-    ap.add_argument("--batch", action="store_true", help="also run the batched 64-instance airfoil sweep")
+    ap.add_argument("--skip-batch", action="store_true", help="skip the batched 64-instance airfoil sweep")
+    ap.add_argument("--skip-warm", action="store_true", help="skip the learned warm start (train + evaluate)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -22,6 +22,16 @@ import numpy as np
 from . import capi
 
 
+def lift_drag(force, mach) -> Tuple[float, float]:
+    """(lift, drag) of a force: its components normal and parallel to the free
+    stream, the normal taken in the x-z plane (mach = M (cos a, 0, sin a))."""
+    m = np.asarray(mach, np.float64)
+    d = m / np.linalg.norm(m)
+    n = np.array([-d[2], 0.0, d[0]])
+    f = np.asarray(force, np.float64)
+    return float(f @ n), float(f @ d)
+
+
 class EulerCase:
     def __init__(self, mesh_path: str, via_fvm: bool = True):
         """Load an SU2 mesh, either through cuMeshFromSu2 + cuMeshFromFile
