@@ -166,18 +166,25 @@ class ClockSampler:
 
 
 def byte_model(case):
-    """Algorithmic bytes per launch of the two hot kernels (each array element
-    of the device layout touched once)."""
-    N, G, F = case.n_cells, case.n_ghosts, case.n_faces
+    """Algorithmic bytes per launch of the two hot kernels: each array element
+    of the device layout that a launch touches, counted once.  Per-face data
+    is stored per cell-face entry (S of them, slot-major); the gradient pass
+    writes the cell's reconstructed state at each face (and each ghost's),
+    which the flux pass reads, its own entries streamed and the neighbour's
+    through the twin index.  k_grad_lim as timed in the per-call loop also
+    stores the gradients and limiters (FvmEulerStepPrepare's outputs)."""
+    N, G = case.n_cells, case.n_ghosts
     S = int(case.mesh.contents._cpu.contents.cell_faces_starts[N])  # interior cell-face entries
     NG = N + G
     state = 4 + 16 + 4          # rho, rhou (float4), rhoe
+    rec = 4 + 16                # reconstructed rho, (rho u, rho E)
     grad_lim = {
-        "cell_geo": 16 * NG, "state": state * NG, "csr": 4 * (N + 1) + 8 * S, "lsq": 32 * N,
-        "face_centre": 16 * F, "grad_write": 80 * N}
+        "cell_geo": 16 * NG, "state": state * NG, "faces_per_cell": N, "lsq": 32 * N,
+        "entry_nbr_weight_face": (4 + 16 + 16 + 4) * S, "ghost_entries": (8 + 16) * G,
+        "face_state_write": rec * (S + G), "grad_write": 80 * N}
     flux = {
-        "cell_geo": 16 * NG, "state": state * NG, "grad": 80 * N, "csr": 4 * (N + 1) + 8 * S,
-        "face_geo": 32 * F, "state_write": state * N, "err_write": 4 * N, "partials": 8 * ((N + 255) // 256)}
+        "cell_volume": 16 * N, "faces_per_cell": N, "entry_twin_normal": (4 + 16) * S, "face_states": rec * (S + G),
+        "state": state * N, "state_write": state * N, "err_write": 4 * N, "partials": 8 * ((N + 255) // 256)}
     return {"k_grad_lim": sum(grad_lim.values()), "k_flux": sum(flux.values()),
             "detail": {"k_grad_lim": grad_lim, "k_flux": flux}, "S": S}
 

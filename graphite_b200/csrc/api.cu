@@ -72,6 +72,7 @@ struct FieldImpl {
     void* val[2] = {nullptr, nullptr};   // float* or float4*
     int cur = 0;
     float4* grad = nullptr;           // N (scalar) or 3N (vector), bound mesh order
+    void* rec = nullptr;              // S + G reconstructed face states: rho (float), rhou (float4 with rho E)
     const cuMesh* bound = nullptr;
     double* partials = nullptr;
     int n_partials = 0;
@@ -102,7 +103,8 @@ void free_mesh(cuMesh* m) {
     MeshImpl* mi = impl(m);
     if (mi) {
         DevMesh& d = mi->dev;
-        dfree(d.cell_geo); dfree(d.face_geo); dfree(d.start); dfree(d.nb); dfree(d.lsq); dfree(d.ghost); dfree(d.red);
+        dfree(d.cell_geo); dfree(d.face_geo); dfree(d.nfc); dfree(d.nb); dfree(d.lsq); dfree(d.ghost); dfree(d.red);
+        dfree(d.twin); dfree(d.cf_geo); dfree(d.nbc); dfree(d.dn); dfree(d.df);
         dfree(mi->d_cell_new);
         delete mi;
     }
@@ -124,7 +126,7 @@ cuMesh* create_mesh(Topology&& topo) {
     number_cells(t, g_renumber.load() != 0, mi->num);
     const Numbering& num = mi->num;
     DevMesh& d = mi->dev;
-    d.N = N; d.G = G; d.F = F; d.S = (int64_t)num.nb_face.size();
+    d.N = N; d.G = G; d.F = F; d.S = kSlots * N;
 
     // float64 metrics in the reference's order
     double *d_nodes = nullptr, *area = nullptr, *normal = nullptr, *fcen = nullptr, *ccen = nullptr, *vol = nullptr,
@@ -145,17 +147,52 @@ cuMesh* create_mesh(Topology&& topo) {
         ok = launch_ok("metric kernels");
     }
     // renumbered float32 layout
-    std::vector<uint2> nb(d.S), gl(G);
-    for (int64_t k = 0; k < d.S; ++k) nb[k] = make_uint2(num.nb_face[k], num.nb_cell[k]);
+    // slot-major per-face entries: (slot t, cell i) at t * N + i
+    std::vector<uint2> nb((size_t)d.S, make_uint2(0, 0)), gl(G);
+    std::vector<uint8_t> nfc((size_t)N);
+    std::vector<uint32_t> twin((size_t)d.S, 0);
+    auto entry = [&](uint32_t cell, uint32_t slot) { return (uint32_t)(slot * N + cell); };
+    for (int64_t i = 0; i < N && ok; ++i) {
+        const uint32_t nf = num.start[i + 1] - num.start[i];
+        if (nf > (uint32_t)kSlots) {
+            set_error("mesh: a cell has more than 6 faces");
+            ok = false;
+            break;
+        }
+        nfc[i] = (uint8_t)nf;
+        for (uint32_t t = 0; t < nf; ++t) {
+            const uint32_t k = num.start[i] + t;
+            nb[entry((uint32_t)i, t)] = make_uint2(num.nb_face[k], num.nb_cell[k]);
+        }
+    }
     for (int64_t g = 0; g < G; ++g) gl[g] = make_uint2(num.ghost_cell[g], num.ghost_face[g]);
+    // twin of each entry: the same face among the neighbour's entries, or the
+    // ghost's slot S + g
+    for (int64_t i = 0; i < N && ok; ++i)
+        for (uint32_t t = 0; t < nfc[i] && ok; ++t) {
+            const uint32_t j = num.nb_cell[num.start[i] + t], f = num.nb_face[num.start[i] + t];
+            uint32_t& tw = twin[entry((uint32_t)i, t)];
+            if (j >= (uint32_t)N) { tw = (uint32_t)(d.S + (j - N)); continue; }
+            tw = UINT32_MAX;
+            for (uint32_t t2 = 0; t2 < num.start[j + 1] - num.start[j]; ++t2)
+                if (num.nb_face[num.start[j] + t2] == f) { tw = entry(j, t2); break; }
+            if (tw == UINT32_MAX) {
+                set_error("mesh: face " + std::to_string(f) + " missing from a neighbour's face list");
+                ok = false;
+            }
+        }
     ok = ok && upload(d_cell_old, num.cell_old, "upload numbering") && upload(d_face_old, num.face_old, "upload numbering") &&
          upload(mi->d_cell_new, num.cell_new, "upload numbering") && dalloc(d.cell_geo, NG, "alloc mesh") &&
-         dalloc(d.face_geo, 2 * F, "alloc mesh") && upload(d.start, num.start, "upload csr") &&
-         upload(d.nb, nb, "upload csr") && dalloc(d.lsq, 2 * N, "alloc mesh") && upload(d.ghost, gl, "upload ghosts");
+         dalloc(d.face_geo, 2 * F, "alloc mesh") && upload(d.nfc, nfc, "upload csr") &&
+         upload(d.nb, nb, "upload csr") && dalloc(d.lsq, 2 * N, "alloc mesh") && upload(d.ghost, gl, "upload ghosts") &&
+         upload(d.twin, twin, "upload csr") && dalloc(d.cf_geo, (size_t)d.S, "alloc mesh") &&
+         dalloc(d.nbc, (size_t)d.S, "alloc mesh") && dalloc(d.dn, (size_t)d.S, "alloc mesh") &&
+         dalloc(d.df, (size_t)d.S, "alloc mesh");
     d.n_red_max = std::max<int>(reduce_blocks(NG), (int)((N + kBlock - 1) / kBlock));
     ok = ok && dalloc(d.red, (size_t)d.n_red_max + 1, "alloc reduction");
     if (ok) {
         launch_layout(d, d_cell_old, d_face_old, area, normal, fcen, ccen, vol, minv, s);
+        launch_entry_geo(d, s);
         ok = launch_ok("layout kernels");
     }
     // host mirror in the reference's layout and order
@@ -247,10 +284,17 @@ bool bind(cuMesh* mesh, FvmField* f, int comps, const char* what) {
 
 bool ensure_grad(cuMesh* mesh, FvmField* f) {
     FieldImpl* fi = impl(f);
-    if (fi->grad) return true;
-    const int64_t N = impl(mesh)->topo.N;
-    if (!dalloc(fi->grad, (size_t)N * fi->comps, "alloc gradient")) return false;
-    return cuda_ok(cudaMemsetAsync(fi->grad, 0, (size_t)N * fi->comps * sizeof(float4), t_stream), "zero gradient");
+    if (fi->grad && fi->rec) return true;
+    const DevMesh& d = impl(mesh)->dev;
+    if (!fi->grad && (!dalloc(fi->grad, (size_t)d.N * fi->comps, "alloc gradient") ||
+                      !cuda_ok(cudaMemsetAsync(fi->grad, 0, (size_t)d.N * fi->comps * sizeof(float4), t_stream),
+                               "zero gradient")))
+        return false;
+    uint8_t* r = nullptr;
+    const size_t bytes = (size_t)(d.S + d.G) * (fi->comps == 1 ? sizeof(float) : sizeof(float4));
+    if (!dalloc(r, bytes, "alloc face states")) return false;
+    fi->rec = r;
+    return true;
 }
 
 bool ensure_partials(FieldImpl* fi, int n) {
@@ -310,8 +354,14 @@ void enqueue_farfield(cuMesh* mesh, FvmField* rho, FvmField* rhou, FvmField* rho
                        make_float3(mach.x, mach.y, mach.z), p, t, s);
 }
 
-EulerGrad grad_of(FvmField* rho, FvmField* rhou, FvmField* rhoe) {
-    return EulerGrad{impl(rho)->grad, impl(rhou)->grad, impl(rhoe)->grad};
+// store_gradients = false: only the face states the flux needs are written
+EulerGrad grad_of(FvmField* rho, FvmField* rhou, FvmField* rhoe, bool store_gradients) {
+    return EulerGrad{store_gradients ? impl(rho)->grad : nullptr, store_gradients ? impl(rhou)->grad : nullptr,
+                     store_gradients ? impl(rhoe)->grad : nullptr, (float*)impl(rho)->rec, (float4*)impl(rhou)->rec};
+}
+
+FaceRecs recs_of(FvmField* rho, FvmField* rhou) {
+    return FaceRecs{(const float*)impl(rho)->rec, (const float4*)impl(rhou)->rec};
 }
 
 void enqueue_flux(cuMesh* mesh, FvmField* rho, FvmField* rhou, FvmField* rhoe, FvmField* error, float cfl, int cur,
@@ -319,9 +369,9 @@ void enqueue_flux(cuMesh* mesh, FvmField* rho, FvmField* rhou, FvmField* rhoe, F
     MeshImpl* mi = impl(mesh);
     const int nxt = 1 - cur;
     FieldImpl* ei = impl(error);
-    launch_flux(mi->dev, state_of(rho, rhou, rhoe, cur), grad_of(rho, rhou, rhoe), (float*)impl(rho)->val[nxt],
+    launch_flux(mi->dev, state_of(rho, rhou, rhoe, cur), recs_of(rho, rhou), (float*)impl(rho)->val[nxt],
                 (float4*)impl(rhou)->val[nxt], (float*)impl(rhoe)->val[nxt], (float*)ei->val[ei->cur], ei->partials,
-                cfl, g_transposed.load() != 0, s);
+                cfl, s);
 }
 
 // Reference-order host copy of the current values.
@@ -546,6 +596,7 @@ void FvmFieldFree(FvmField* f) {
     FieldImpl* fi = impl(f);
     if (fi) {
         dfree(fi->val[0]); dfree(fi->val[1]); dfree(fi->grad); dfree(fi->partials); dfree(fi->staging);
+        if (fi->rec) cudaFree(fi->rec);
         delete fi;
     }
     if (f->_cpu) {
@@ -640,7 +691,8 @@ int FvmEulerStepPrepare(cuMesh* mesh, FvmField* rho, FvmField* rhou, FvmField* r
     clear_error();
     if (!euler_fields(mesh, rho, rhou, rhoe, "FvmEulerStepPrepare")) return 1;
     if (!ensure_grad(mesh, rho) || !ensure_grad(mesh, rhou) || !ensure_grad(mesh, rhoe)) return 1;
-    launch_grad_lim(impl(mesh)->dev, state_of(rho, rhou, rhoe, impl(rho)->cur), grad_of(rho, rhou, rhoe), t_stream);
+    launch_grad_lim(impl(mesh)->dev, state_of(rho, rhou, rhoe, impl(rho)->cur), grad_of(rho, rhou, rhoe, true),
+                    g_transposed.load() != 0, t_stream);
     return launch_ok("FvmEulerStepPrepare") ? 0 : 1;
 }
 
@@ -653,7 +705,7 @@ int FvmEulerStep(cuMesh* mesh, FvmField* rho, FvmField* rhou, FvmField* rhoe, gb
         return 1;
     }
     if (!euler_fields(mesh, rho, rhou, rhoe, "FvmEulerStep") || !bind(mesh, error, 1, "FvmEulerStep")) return 1;
-    if (!impl(rho)->grad || !impl(rhou)->grad || !impl(rhoe)->grad) {
+    if (!impl(rho)->rec || !impl(rhou)->rec) {
         set_error("FvmEulerStep: call FvmEulerStepPrepare first");
         return 1;
     }
@@ -733,7 +785,8 @@ int64_t gbEulerRun(cuMesh* mesh, FvmField* rho, FvmField* rhou, FvmField* rhoe, 
             else enqueue_farfield(mesh, rho, rhou, rhoe, (int)bcs[b].region_id, k, bcs[b].mach, bcs[b].pressure,
                                   bcs[b].temperature, cap);
         }
-        launch_grad_lim(mi->dev, state_of(rho, rhou, rhoe, k), grad_of(rho, rhou, rhoe), cap);
+        launch_grad_lim(mi->dev, state_of(rho, rhou, rhoe, k), grad_of(rho, rhou, rhoe, false),
+                        g_transposed.load() != 0, cap);
         enqueue_flux(mesh, rho, rhou, rhoe, error, cfl, k, cap);
         launch_reduce_final(nb, ei->partials, out, d_hist, d_counter, cap);
         ok = cuda_ok(cudaStreamEndCapture(cap, &g), "graph capture") &&

@@ -33,9 +33,8 @@ struct InstDev {
     float* rho[2];
     float4* rhou[2];
     float* rhoe[2];
-    float4* g_rho;
-    float4* g_rhou;
-    float4* g_rhoe;
+    float* rec_rho;       // reconstructed face states, S + G: rho
+    float4* rec_rhou;     // (rho u, rho E)
     double* partials;     // one per cell tile
     double* hist;         // residual per iteration of the current run
     int mesh;
@@ -67,8 +66,8 @@ struct BcDev {
 // 256-thread blocks per SM): variant 0 keeps every value in registers,
 // variant 1 trades a few spills for one more resident block.  The autotuner
 // picks one.
-constexpr int kBatchGradBlocks[2] = {3, 4};
-constexpr int kBatchFluxBlocks[2] = {2, 3};
+constexpr int kBatchGradBlocks[2] = {4, 5};
+constexpr int kBatchFluxBlocks[2] = {4, 5};
 
 __global__ void k_batch_bc(const int2* __restrict__ items, int n_items, InstDev* insts,
                            const MeshTab* __restrict__ meshes, const BcDev* __restrict__ bcs) {
@@ -99,7 +98,7 @@ __global__ void k_batch_bc(const int2* __restrict__ items, int n_items, InstDev*
     }
 }
 
-template <int BLOCKS>
+template <bool TRANSPOSED, int BLOCKS>
 __global__ void __launch_bounds__(kBlock, BLOCKS)
     k_batch_grad(const int2* __restrict__ items, const InstDev* insts, const MeshTab* __restrict__ meshes, int tile) {
     const int2 w = items[blockIdx.x];
@@ -108,13 +107,13 @@ __global__ void __launch_bounds__(kBlock, BLOCKS)
     const MeshDev m = meshes[I.mesh].m;
     const int cur = I.cur;
     const EulerState q{I.rho[cur], I.rhou[cur], I.rhoe[cur]};
-    const EulerGrad g{I.g_rho, I.g_rhou, I.g_rhoe};
+    const EulerGrad g{nullptr, nullptr, nullptr, I.rec_rho, I.rec_rhou};
     const uint32_t c0 = (uint32_t)w.y * tile;
     const uint32_t c1 = min(m.N, c0 + (uint32_t)tile);
-    for (uint32_t i = c0 + threadIdx.x; i < c1; i += blockDim.x) grad_lim_cell(m, q, g, i);
+    for (uint32_t i = c0 + threadIdx.x; i < c1; i += blockDim.x) grad_lim_cell<TRANSPOSED>(m, q, g, i);
 }
 
-template <bool TRANSPOSED, int BLOCKS>
+template <int BLOCKS>
 __global__ void __launch_bounds__(kBlock, BLOCKS)
     k_batch_flux(const int2* __restrict__ items, const InstDev* insts, const MeshTab* __restrict__ meshes, int tile,
                  float cfl) {
@@ -128,8 +127,8 @@ __global__ void __launch_bounds__(kBlock, BLOCKS)
     const uint32_t c1 = min(m.N, c0 + (uint32_t)tile);
     double res = 0.0;
     for (uint32_t i = c0 + threadIdx.x; i < c1; i += blockDim.x)
-        res += (double)flux_cell<TRANSPOSED>(m, q, I.g_rho, I.g_rhou, I.g_rhoe, I.rho[nxt], I.rhou[nxt], I.rhoe[nxt],
-                                             nullptr, cfl, i);
+        res += (double)flux_cell(m, q, FaceRecs{I.rec_rho, I.rec_rhou}, I.rho[nxt], I.rhou[nxt], I.rhoe[nxt],
+                                 nullptr, cfl, i);
     const double bs = block_sum(res);
     if (threadIdx.x == 0) I.partials[w.y] = bs;
 }
@@ -295,13 +294,13 @@ void enqueue_iteration(Batch* b, float cfl, double tol, cudaStream_t s) {
         const int n = b->n_cell_items;
         const bool tr = reference_momentum();
         if (b->variant == 0) {
-            k_batch_grad<kBatchGradBlocks[0]><<<n, kBlock, 0, s>>>(b->d_cell_items, b->d_inst, b->d_mesh, b->tile);
-            if (tr) k_batch_flux<true, kBatchFluxBlocks[0]><<<n, kBlock, 0, s>>>(b->d_cell_items, b->d_inst, b->d_mesh, b->tile, cfl);
-            else k_batch_flux<false, kBatchFluxBlocks[0]><<<n, kBlock, 0, s>>>(b->d_cell_items, b->d_inst, b->d_mesh, b->tile, cfl);
+            if (tr) k_batch_grad<true, kBatchGradBlocks[0]><<<n, kBlock, 0, s>>>(b->d_cell_items, b->d_inst, b->d_mesh, b->tile);
+            else k_batch_grad<false, kBatchGradBlocks[0]><<<n, kBlock, 0, s>>>(b->d_cell_items, b->d_inst, b->d_mesh, b->tile);
+            k_batch_flux<kBatchFluxBlocks[0]><<<n, kBlock, 0, s>>>(b->d_cell_items, b->d_inst, b->d_mesh, b->tile, cfl);
         } else {
-            k_batch_grad<kBatchGradBlocks[1]><<<n, kBlock, 0, s>>>(b->d_cell_items, b->d_inst, b->d_mesh, b->tile);
-            if (tr) k_batch_flux<true, kBatchFluxBlocks[1]><<<n, kBlock, 0, s>>>(b->d_cell_items, b->d_inst, b->d_mesh, b->tile, cfl);
-            else k_batch_flux<false, kBatchFluxBlocks[1]><<<n, kBlock, 0, s>>>(b->d_cell_items, b->d_inst, b->d_mesh, b->tile, cfl);
+            if (tr) k_batch_grad<true, kBatchGradBlocks[1]><<<n, kBlock, 0, s>>>(b->d_cell_items, b->d_inst, b->d_mesh, b->tile);
+            else k_batch_grad<false, kBatchGradBlocks[1]><<<n, kBlock, 0, s>>>(b->d_cell_items, b->d_inst, b->d_mesh, b->tile);
+            k_batch_flux<kBatchFluxBlocks[1]><<<n, kBlock, 0, s>>>(b->d_cell_items, b->d_inst, b->d_mesh, b->tile, cfl);
         }
     }
     k_batch_reduce<<<b->n_inst, kBlock, 0, s>>>(b->d_inst, tol);
@@ -394,8 +393,9 @@ gbBatch* gbBatchCreate(int n_meshes, cuMesh* const* meshes, int n_instances, con
         ok = balloc(b, d, reg.size(), "batch regions") &&
              ok_(cudaMemcpyAsync(d, reg.data(), reg.size(), cudaMemcpyHostToDevice, s), "batch regions");
         const DevMesh& D = *A.dev;
-        tabs[m] = MeshTab{MeshDev{D.cell_geo, D.face_geo, D.start, D.nb, D.lsq, (uint32_t)D.N}, D.ghost, d,
-                          (uint32_t)D.G};
+        tabs[m] = MeshTab{MeshDev{D.cell_geo, D.face_geo, D.nfc, D.nb, D.lsq, D.twin, D.cf_geo, D.nbc, D.dn, D.df,
+                                  (uint32_t)D.N, (uint32_t)D.S},
+                          D.ghost, d, (uint32_t)D.G};
         b->signature += std::to_string(A.N) + "/";
     }
     ok = ok && balloc(b, b->d_mesh, n_meshes, "batch meshes") &&
@@ -430,8 +430,8 @@ gbBatch* gbBatchCreate(int n_meshes, cuMesh* const* meshes, int n_instances, con
         for (int k = 0; k < 2 && ok; ++k)
             ok = balloc(b, I.rho[k], NG, "batch state") && balloc(b, I.rhou[k], NG, "batch state") &&
                  balloc(b, I.rhoe[k], NG, "batch state");
-        ok = ok && balloc(b, I.g_rho, A.N, "batch gradients") && balloc(b, I.g_rhou, 3 * A.N, "batch gradients") &&
-             balloc(b, I.g_rhoe, A.N, "batch gradients");
+        const int64_t SG = A.dev->S + A.G;
+        ok = ok && balloc(b, I.rec_rho, SG, "batch face states") && balloc(b, I.rec_rhou, SG, "batch face states");
     }
     for (int m = 0; m < n_meshes; ++m) b->signature += std::to_string(per_mesh[m]) + ",";
     ok = ok && balloc(b, b->d_bcs, b->h_bcs.size(), "batch bcs") &&

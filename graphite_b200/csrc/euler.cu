@@ -7,10 +7,14 @@
 // Both hot kernels are cell-gathers over the renumbered (reverse
 // Cuthill-McKee) mesh: one thread per interior cell walks its faces in the
 // reference's element-local order, so every sum is taken in the reference's
-// order and no atomics are used -- runs are bitwise reproducible.  They are
-// HBM-bandwidth bound: per cell and iteration they stream the cell's own
-// record once and gather neighbour records that the renumbering keeps
-// resident in L2.
+// order and no atomics are used -- runs are bitwise reproducible.  Per-face
+// data is stored slot-major (face slot t of cell i at t * N + i), so a warp
+// reads and writes it coalesced.  The gradient pass streams the static face
+// geometry, gathers the neighbours' states and writes, per face entry, the
+// cell's limited reconstruction at that face; the flux pass streams its own
+// entries (twin index, oriented normal with area / volume, reconstructed
+// state) and gathers only the neighbour's 20-byte reconstructed state through
+// the twin index.
 #include "euler_ops.cuh"
 
 namespace gb {
@@ -19,10 +23,10 @@ namespace {
 // Resident blocks per SM the two hot kernels are compiled for (register
 // budget 65536 / (kBlock * blocks)).
 #ifndef GB_FLUX_BLOCKS
-#define GB_FLUX_BLOCKS 3
+#define GB_FLUX_BLOCKS 6
 #endif
 #ifndef GB_GRAD_BLOCKS
-#define GB_GRAD_BLOCKS 4
+#define GB_GRAD_BLOCKS 5
 #endif
 constexpr int kFluxBlocksPerSM = GB_FLUX_BLOCKS;
 constexpr int kGradBlocksPerSM = GB_GRAD_BLOCKS;
@@ -74,27 +78,30 @@ __global__ void k_bc_farfield(uint32_t g0, uint32_t g1, uint32_t N, const float4
     }
 }
 
-// Fused FvmEulerStepPrepare over the interior cells of one mesh.
+// Fused FvmEulerStepPrepare over the interior cells of one mesh: gradients,
+// limiters and the reconstructed face states.
+template <bool TRANSPOSED>
 __global__ void __launch_bounds__(kBlock, kGradBlocksPerSM) k_grad_lim(MeshDev m, EulerState q, EulerGrad g) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < m.N) grad_lim_cell(m, q, g, i);
+    if (i < m.N) grad_lim_cell<TRANSPOSED>(m, q, g, i);
 }
 
 // Fused flux / local-time-step update / squared residual over the interior
 // cells of one mesh, with the residual summed per block in float64.
-template <bool TRANSPOSED>
-__global__ void __launch_bounds__(kBlock, kFluxBlocksPerSM) k_flux(MeshDev m, EulerState q,
-                                                                   const float4* __restrict__ g_rho,
-                                                                   const float4* __restrict__ g_rhou,
-                                                                   const float4* __restrict__ g_rhoe,
-                                                                   float* __restrict__ rho_n, float4* __restrict__ rhou_n,
-                                                                   float* __restrict__ rhoe_n, float* __restrict__ err,
-                                                                   double* __restrict__ partials, float cfl) {
+__global__ void __launch_bounds__(kBlock, kFluxBlocksPerSM)
+    k_flux(MeshDev m, EulerState q, FaceRecs r, float* __restrict__ rho_n, float4* __restrict__ rhou_n,
+           float* __restrict__ rhoe_n, float* __restrict__ err, double* __restrict__ partials, float cfl) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     double res = 0.0;
-    if (i < m.N) res = (double)flux_cell<TRANSPOSED>(m, q, g_rho, g_rhou, g_rhoe, rho_n, rhou_n, rhoe_n, err, cfl, i);
+    if (i < m.N) res = (double)flux_cell(m, q, r, rho_n, rhou_n, rhoe_n, err, cfl, i);
     const double bs = block_sum(res);
     if (threadIdx.x == 0) partials[blockIdx.x] = bs;
+}
+
+// one-off setup of the static per-entry geometry
+__global__ void k_entry_geo(MeshDev m, float4* cf_geo, uint32_t* nbc, float4* dn, float4* df) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < m.N) entry_geo_cell(m, cf_geo, nbc, dn, df, i);
 }
 
 __global__ void k_reduce_partials(int64_t n, const float* __restrict__ v, double* partials) {
@@ -174,24 +181,27 @@ void launch_bc_farfield(const DevMesh& m, uint32_t g0, uint32_t g1, float* rho[2
 }
 
 MeshDev mesh_dev(const DevMesh& m) {
-    return MeshDev{m.cell_geo, m.face_geo, m.start, m.nb, m.lsq, (uint32_t)m.N};
+    return MeshDev{m.cell_geo, m.face_geo, m.nfc, m.nb, m.lsq, m.twin, m.cf_geo, m.nbc, m.dn, m.df,
+                   (uint32_t)m.N, (uint32_t)m.S};
 }
 
-void launch_grad_lim(const DevMesh& m, EulerState q, EulerGrad g, cudaStream_t s) {
+void launch_entry_geo(const DevMesh& m, cudaStream_t s) {
     if (m.N == 0) return;
-    k_grad_lim<<<grid(m.N), kBlock, 0, s>>>(mesh_dev(m), q, g);
+    k_entry_geo<<<grid(m.N), kBlock, 0, s>>>(mesh_dev(m), m.cf_geo, m.nbc, m.dn, m.df);
     count_launch();
 }
 
-void launch_flux(const DevMesh& m, EulerState q, EulerGrad g, float* rho_n, float4* rhou_n, float* rhoe_n,
-                 float* err, double* partials, float cfl, bool transposed, cudaStream_t s) {
+void launch_grad_lim(const DevMesh& m, EulerState q, EulerGrad g, bool transposed, cudaStream_t s) {
     if (m.N == 0) return;
-    if (transposed)
-        k_flux<true><<<grid(m.N), kBlock, 0, s>>>(mesh_dev(m), q, g.rho, g.rhou, g.rhoe, rho_n, rhou_n, rhoe_n, err,
-                                                  partials, cfl);
-    else
-        k_flux<false><<<grid(m.N), kBlock, 0, s>>>(mesh_dev(m), q, g.rho, g.rhou, g.rhoe, rho_n, rhou_n, rhoe_n, err,
-                                                   partials, cfl);
+    if (transposed) k_grad_lim<true><<<grid(m.N), kBlock, 0, s>>>(mesh_dev(m), q, g);
+    else k_grad_lim<false><<<grid(m.N), kBlock, 0, s>>>(mesh_dev(m), q, g);
+    count_launch();
+}
+
+void launch_flux(const DevMesh& m, EulerState q, FaceRecs r, float* rho_n, float4* rhou_n, float* rhoe_n,
+                 float* err, double* partials, float cfl, cudaStream_t s) {
+    if (m.N == 0) return;
+    k_flux<<<grid(m.N), kBlock, 0, s>>>(mesh_dev(m), q, r, rho_n, rhou_n, rhoe_n, err, partials, cfl);
     count_launch();
 }
 

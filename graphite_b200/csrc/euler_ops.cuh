@@ -10,10 +10,16 @@ namespace gb {
 struct MeshDev {
     const float4* cell_geo;
     const float4* face_geo;
-    const uint32_t* start;
+    const uint8_t* nfc;
     const uint2* nb;
     const float4* lsq;
+    const uint32_t* twin;
+    const float4* cf_geo;
+    const uint32_t* nbc;
+    const float4* dn;
+    const float4* df;
     uint32_t N;
+    uint32_t S;
 };
 
 __device__ __forceinline__ float3 f3(float4 a) { return make_float3(a.x, a.y, a.z); }
@@ -163,29 +169,35 @@ __device__ __forceinline__ void farfield_ghost(const float4* __restrict__ cell_g
 
 // Fused FvmEulerStepPrepare for one interior cell i (src/models/euler.cu:597-647):
 // least-squares gradients (src/fvmops.cu:51-111) and limiters
-// (src/fvmops.cu:175-266) of rho, rhou (3 components) and rhoE in one pass
-// over the cell's faces.
+// (src/fvmops.cu:175-266) of rho, rhou (3 components) and rhoE, then the
+// limited reconstruction q + lim (grad q . d) of the cell at each of its faces
+// (the face states of fvmEulerSteadyOp, src/models/euler.cu:250-255) and of
+// each ghost neighbour, which carries this cell's gradient and limiter
+// (fvmScalGradLimBc / fvmVecGradLimBc, src/fvmops.cu:272-304).
+template <bool TRANSPOSED>
 __device__ __forceinline__ void grad_lim_cell(const MeshDev& m, EulerState q, EulerGrad g, uint32_t i) {
     const float3 ci = f3(__ldg(&m.cell_geo[i]));
     float v[5];
+    float4 u0;
     {
-        const float4 u = __ldg(&q.rhou[i]);
-        v[0] = __ldg(&q.rho[i]); v[1] = u.x; v[2] = u.y; v[3] = u.z; v[4] = __ldg(&q.rhoe[i]);
+        u0 = __ldg(&q.rhou[i]);
+        v[0] = __ldg(&q.rho[i]); v[1] = u0.x; v[2] = u0.y; v[3] = u0.z; v[4] = __ldg(&q.rhoe[i]);
     }
     float3 gs[5];
     float vmin[5], vmax[5];
 #pragma unroll
     for (int c = 0; c < 5; ++c) { gs[c] = make_float3(0.f, 0.f, 0.f); vmin[c] = v[c]; vmax[c] = v[c]; }
-    const uint32_t s0 = __ldg(&m.start[i]), s1 = __ldg(&m.start[i + 1]);
-    for (uint32_t k = s0; k < s1; ++k) {
-        const uint32_t j = __ldg(&m.nb[k]).y;
-        const float3 d = f3(__ldg(&m.cell_geo[j])) - ci;
-        const float w2 = 1.f / dot(d, d);
+    const uint32_t nf = __ldg(&m.nfc[i]);
+    const uint32_t kend = i + nf * m.N;
+    for (uint32_t k = i; k < kend; k += m.N) {
+        const uint32_t j = __ldg(&m.nbc[k]);
+        const float4 dw = __ldg(&m.dn[k]);           // (c_j - c_i, 1 / |c_j - c_i|^2)
+        const float3 d = f3(dw);
         const float4 uj = __ldg(&q.rhou[j]);
         const float vj[5] = {__ldg(&q.rho[j]), uj.x, uj.y, uj.z, __ldg(&q.rhoe[j])};
 #pragma unroll
         for (int c = 0; c < 5; ++c) {
-            gs[c] = gs[c] + (d * (vj[c] - v[c])) * w2;
+            gs[c] = gs[c] + (d * (vj[c] - v[c])) * dw.w;
             vmin[c] = fminf(vmin[c], vj[c]);
             vmax[c] = fmaxf(vmax[c], vj[c]);
         }
@@ -194,74 +206,66 @@ __device__ __forceinline__ void grad_lim_cell(const MeshDev& m, EulerState q, Eu
 #pragma unroll
     for (int c = 0; c < 5; ++c) gs[c] = sym_mul(l0, l1, gs[c]);
     float lim[5] = {2.f, 2.f, 2.f, 2.f, 2.f};
-    for (uint32_t k = s0; k < s1; ++k) {
-        const uint32_t f = __ldg(&m.nb[k]).x;
-        const float3 d = f3(__ldg(&m.face_geo[2 * f + 1])) - ci;
-        const float dn = norm(d);
-        const float k3 = dn * dn * dn;
+    for (uint32_t k = i; k < kend; k += m.N) {
+        const float4 dk = __ldg(&m.df[k]);           // (f_c - c_i, |f_c - c_i|^3)
 #pragma unroll
-        for (int c = 0; c < 5; ++c) lim[c] = fminf(lim[c], limiter(v[c], gs[c], vmin[c], vmax[c], d, k3));
+        for (int c = 0; c < 5; ++c) lim[c] = fminf(lim[c], limiter(v[c], gs[c], vmin[c], vmax[c], f3(dk), dk.w));
     }
-    g.rho[i] = make_float4(gs[0].x, gs[0].y, gs[0].z, lim[0]);
-    g.rhou[3 * i] = make_float4(gs[1].x, gs[1].y, gs[1].z, lim[1]);
-    g.rhou[3 * i + 1] = make_float4(gs[2].x, gs[2].y, gs[2].z, lim[2]);
-    g.rhou[3 * i + 2] = make_float4(gs[3].x, gs[3].y, gs[3].z, lim[3]);
-    g.rhoe[i] = make_float4(gs[4].x, gs[4].y, gs[4].z, lim[4]);
+    const float4 gr = make_float4(gs[0].x, gs[0].y, gs[0].z, lim[0]);
+    const float4 gu[3] = {make_float4(gs[1].x, gs[1].y, gs[1].z, lim[1]),
+                          make_float4(gs[2].x, gs[2].y, gs[2].z, lim[2]),
+                          make_float4(gs[3].x, gs[3].y, gs[3].z, lim[3])};
+    const float4 ge = make_float4(gs[4].x, gs[4].y, gs[4].z, lim[4]);
+    if (g.rho) {
+        g.rho[i] = gr;
+        g.rhou[3 * i] = gu[0];
+        g.rhou[3 * i + 1] = gu[1];
+        g.rhou[3 * i + 2] = gu[2];
+        g.rhoe[i] = ge;
+    }
+    for (uint32_t k = i; k < kend; k += m.N) {
+        float rr, re;
+        float3 ru;
+        reconstruct<TRANSPOSED>(v[0], u0, v[4], gr, gu, ge, f3(__ldg(&m.df[k])), rr, ru, re);
+        g.rec_rho[k] = rr;
+        g.rec_rhou[k] = make_float4(ru.x, ru.y, ru.z, re);
+        const uint32_t t = __ldg(&m.twin[k]);
+        if (t >= m.S) {
+            // ghost neighbour: its state with this cell's gradient and limiter
+            const uint32_t j = m.N + (t - m.S);
+            const float3 fc = f3(__ldg(&m.face_geo[2 * __ldg(&m.nb[k]).x + 1]));
+            reconstruct<TRANSPOSED>(__ldg(&q.rho[j]), __ldg(&q.rhou[j]), __ldg(&q.rhoe[j]), gr, gu, ge,
+                                    fc - f3(__ldg(&m.cell_geo[j])), rr, ru, re);
+            g.rec_rho[t] = rr;
+            g.rec_rhou[t] = make_float4(ru.x, ru.y, ru.z, re);
+        }
+    }
 }
 
 // Fused fvmEulerSteadyOp + euler_steady_step for one interior cell i
-// (src/models/euler.cu:236-381): per face, reconstruct both sides, central
+// (src/models/euler.cu:236-381): per face, from the two reconstructed face
+// states (this cell's, and the neighbour's through the twin entry), central
 // flux 0.5 (F0 + F1) . n A / V minus scalar dissipation 0.5 eig (q1 - q0) A / V
 // with eig = max(|u| + c) over both sides, accumulate eig A / V; then
 // dt = cfl / sum, q_new = q - F dt (into the other buffer).  Returns the
 // squared residual (F_rho^2 + |F_rhou|^2 + F_rhoE^2) V, also stored in err[i]
 // when err is not null.
-template <bool TRANSPOSED>
-__device__ __forceinline__ float flux_cell(const MeshDev& m, EulerState q, const float4* __restrict__ g_rho,
-                                           const float4* __restrict__ g_rhou, const float4* __restrict__ g_rhoe,
-                                           float* __restrict__ rho_n, float4* __restrict__ rhou_n,
-                                           float* __restrict__ rhoe_n, float* __restrict__ err, float cfl,
-                                           uint32_t i) {
-    const uint32_t N = m.N;
-    const float4 c0 = __ldg(&m.cell_geo[i]);
-    const float3 ci = f3(c0);
-    const float inv_v = 1.f / c0.w;
-    const float r0 = __ldg(&q.rho[i]);
-    const float4 u0 = __ldg(&q.rhou[i]);
-    const float e0 = __ldg(&q.rhoe[i]);
-    const float4 gr0 = __ldg(&g_rho[i]), ge0 = __ldg(&g_rhoe[i]);
-    const float4 gu0[3] = {__ldg(&g_rhou[3 * i]), __ldg(&g_rhou[3 * i + 1]), __ldg(&g_rhou[3 * i + 2])};
+__device__ __forceinline__ float flux_cell(const MeshDev& m, EulerState q, FaceRecs rec, float* __restrict__ rho_n,
+                                           float4* __restrict__ rhou_n, float* __restrict__ rhoe_n,
+                                           float* __restrict__ err, float cfl, uint32_t i) {
+    const float vol = __ldg(&m.cell_geo[i]).w;
     float fr = 0.f, fe = 0.f, dts = 0.f;
     float3 fu = make_float3(0.f, 0.f, 0.f);
-    const uint32_t s0 = __ldg(&m.start[i]), s1 = __ldg(&m.start[i + 1]);
-    for (uint32_t k = s0; k < s1; ++k) {
-        const uint2 fj = __ldg(&m.nb[k]);
-        const uint32_t f = fj.x, j = fj.y;
-        const float4 na = __ldg(&m.face_geo[2 * f]);
-        const float3 fc = f3(__ldg(&m.face_geo[2 * f + 1]));
-        const float3 d0 = fc - ci;
-        const float3 d1 = fc - f3(__ldg(&m.cell_geo[j]));
-        const float3 n = outer_normal(f3(na), d0);
-        const float ds = na.w * inv_v;
-        const float r1 = __ldg(&q.rho[j]);
-        const float4 u1 = __ldg(&q.rhou[j]);
-        const float e1 = __ldg(&q.rhoe[j]);
-        float4 gr1, ge1, gu1[3];
-        if (j < N) {
-            gr1 = __ldg(&g_rho[j]);
-            ge1 = __ldg(&g_rhoe[j]);
-            gu1[0] = __ldg(&g_rhou[3 * j]);
-            gu1[1] = __ldg(&g_rhou[3 * j + 1]);
-            gu1[2] = __ldg(&g_rhou[3 * j + 2]);
-        } else {
-            // a ghost carries its interior cell's gradient and limiter
-            // (fvmScalGradLimBc / fvmVecGradLimBc, src/fvmops.cu:272-304)
-            gr1 = gr0; ge1 = ge0; gu1[0] = gu0[0]; gu1[1] = gu0[1]; gu1[2] = gu0[2];
-        }
-        float ra, rb, ea, eb;
-        float3 ua, ub;
-        reconstruct<TRANSPOSED>(r0, u0, e0, gr0, gu0, ge0, d0, ra, ua, ea);
-        reconstruct<TRANSPOSED>(r1, u1, e1, gr1, gu1, ge1, d1, rb, ub, eb);
+    const uint32_t nf = __ldg(&m.nfc[i]);
+    for (uint32_t k = i; k < i + nf * m.N; k += m.N) {
+        const uint32_t t = __ldg(&m.twin[k]);
+        const float4 gk = __ldg(&m.cf_geo[k]);
+        const float3 n = f3(gk);
+        const float ds = gk.w;
+        const float ra = __ldg(&rec.rho[k]), rb = __ldg(&rec.rho[t]);
+        const float4 uea = __ldg(&rec.rhou[k]), ueb = __ldg(&rec.rhou[t]);   // (rho u, rho E)
+        const float3 ua = f3(uea), ub = f3(ueb);
+        const float ea = uea.w, eb = ueb.w;
         // one reciprocal of the density per side, reused by every quotient
         const float ia = 1.f / ra, ib = 1.f / rb;
         const float qa = dot(ua, ua), qb = dot(ub, ub);
@@ -273,21 +277,49 @@ __device__ __forceinline__ float flux_cell(const MeshDev& m, EulerState q, const
         fr += (va * ra + vb * rb) * h;
         fu = fu + ((ua * va + n * pa) + (ub * vb + n * pb)) * h;
         fe += (va * (ea + pa) + vb * (eb + pb)) * h;
-        const float eig = fmaxf(sqrtf(qa) * ia + lsqrt(1.4f * pa * ia),
-                                sqrtf(qb) * ib + lsqrt(1.4f * pb * ib));
+        const float eig = fmaxf(sqrtf(qa) * ia + lsqrt(1.4f * pa * ia), sqrtf(qb) * ib + lsqrt(1.4f * pb * ib));
         const float eh = eig * h;
         fr -= eh * (rb - ra);
         fu = fu - (ub - ua) * eh;
         fe -= eh * (eb - ea);
         dts += eig * ds;
     }
+    const float r0 = __ldg(&q.rho[i]);
+    const float4 u0 = __ldg(&q.rhou[i]);
+    const float e0 = __ldg(&q.rhoe[i]);
     const float dt = cfl / dts;
     rho_n[i] = r0 - fr * dt;
     rhou_n[i] = make_float4(u0.x - fu.x * dt, u0.y - fu.y * dt, u0.z - fu.z * dt, 0.f);
     rhoe_n[i] = e0 - fe * dt;
-    const float e = (fr * fr + dot(fu, fu) + fe * fe) * c0.w;
+    const float e = (fr * fr + dot(fu, fu) + fe * fe) * vol;
     if (err) err[i] = e;
     return e;
+}
+
+// The static per-entry geometry of cell i, computed with the arithmetic the
+// iteration would otherwise repeat every step: for the flux the face normal
+// oriented away from the cell (outer_normal) and the face area over the cell
+// volume; for the gradient the neighbour offset with its LSQ weight
+// 1 / |d|^2 and the face offset with the limiter's |d|^3.
+__device__ __forceinline__ void entry_geo_cell(const MeshDev& m, float4* cf_geo, uint32_t* nbc, float4* dn,
+                                               float4* df, uint32_t i) {
+    const float4 c0 = __ldg(&m.cell_geo[i]);
+    const float3 ci = f3(c0);
+    const float inv_v = 1.f / c0.w;
+    const uint32_t nf = __ldg(&m.nfc[i]);
+    for (uint32_t k = i; k < i + nf * m.N; k += m.N) {
+        const uint2 fj = __ldg(&m.nb[k]);
+        const float4 na = __ldg(&m.face_geo[2 * fj.x]);
+        const float3 fd = f3(__ldg(&m.face_geo[2 * fj.x + 1])) - ci;
+        const float3 n = outer_normal(f3(na), fd);
+        cf_geo[k] = make_float4(n.x, n.y, n.z, na.w * inv_v);
+        const float3 d = f3(__ldg(&m.cell_geo[fj.y])) - ci;
+        const float w2 = 1.f / dot(d, d);
+        dn[k] = make_float4(d.x, d.y, d.z, w2);
+        const float dl = norm(fd);
+        df[k] = make_float4(fd.x, fd.y, fd.z, dl * dl * dl);
+        nbc[k] = fj.y;
+    }
 }
 
 }  // namespace gb

@@ -3,16 +3,29 @@
 // Layout in HBM (all indices uint32, new = renumbered order):
 //   cell_geo  float4[N+G]   centroid xyz, volume            (interior, then ghosts)
 //   face_geo  float4[2F]    (unit normal xyz, area), (face centre xyz, 0)
-//   start     uint32[N+1]   interior cell -> first CSR entry
-//   nb        uint2[S]      (face, neighbour cell) per interior cell face, in
-//                           the reference's element-local face order
 //   lsq       float4[2N]    inverse LSQ matrix, symmetric: (a00 a01 a02 a11), (a12 a22 - -)
 //   ghost     uint2[G]      (interior cell, face) of each ghost
+//   nfc       uint8[N]      faces of each interior cell (at most kSlots = 6)
+// Per-face entries are slot-major: entry (slot t, cell i) at t * N + i, slot
+// t = the cell's t-th face in the reference's element-local face order, so a
+// warp's threads (consecutive cells) touch consecutive entries.  S = 6 N.
+//   nb        uint2[S]      (face, neighbour cell)
+//   twin      uint32[S]     the entry of the same face among the neighbour's
+//                           entries, or S + g for a ghost neighbour N + g
+//   cf_geo    float4[S]     face normal oriented away from the cell, area /
+//                           cell volume
+//   nbc       uint32[S]     neighbour cell
+//   dn        float4[S]     neighbour centroid - cell centroid, 1 / |.|^2
+//   df        float4[S]     face centre - cell centroid, |.|^3
 // Fields (double-buffered values so that the update is a Jacobi sweep):
 //   scalar    float [N+G] x2
 //   vector    float4[N+G] x2 (xyz, pad)
 //   gradient  scalar: float4[N] (gradient xyz, limiter)
 //             vector: float4[3N], entry 3i+a = (gradient of component a, its limiter)
+//   face rec  float[S+G] (rho) and float4[S+G] (rho u, rho E), owned by the
+//             rho and rhou fields: the limited reconstruction of the cell's
+//             state at each of its faces (per entry), then of each ghost's
+//             state at its face (S + g)
 #pragma once
 
 #include <cuda_runtime.h>
@@ -24,13 +37,18 @@
 namespace gb {
 
 struct DevMesh {
-    int64_t N = 0, G = 0, F = 0, S = 0;
+    int64_t N = 0, G = 0, F = 0, S = 0;   // S = kSlots * N per-face entries
     float4* cell_geo = nullptr;
     float4* face_geo = nullptr;
-    uint32_t* start = nullptr;
+    uint8_t* nfc = nullptr;
     uint2* nb = nullptr;
     float4* lsq = nullptr;
     uint2* ghost = nullptr;
+    uint32_t* twin = nullptr;
+    float4* cf_geo = nullptr;
+    uint32_t* nbc = nullptr;
+    float4* dn = nullptr;
+    float4* df = nullptr;
     // reduction scratch owned by the mesh
     double* red = nullptr;        // n_red_max partials + 1 result
     int n_red_max = 0;
@@ -43,13 +61,23 @@ struct EulerState {
     const float* rhoe;
 };
 
+// Outputs of the gradient / limiter pass: the gradients (may be null, then
+// they are not stored) and the reconstructed face states the flux reads.
 struct EulerGrad {
-    float4* rho;     // N
-    float4* rhou;    // 3N
-    float4* rhoe;    // N
+    float4* rho;       // N
+    float4* rhou;      // 3N
+    float4* rhoe;      // N
+    float* rec_rho;    // S + G: reconstructed rho
+    float4* rec_rhou;  // S + G: reconstructed (rho u, rho E)
+};
+
+struct FaceRecs {
+    const float* rho;
+    const float4* rhou;   // (rho u, rho E)
 };
 
 constexpr int kBlock = 256;
+constexpr int kSlots = 6;   // faces per cell: tet 4, prism / pyramid 5, hex 6
 
 int reduce_blocks(int64_t n);
 
@@ -74,9 +102,10 @@ void launch_bc_slip(const DevMesh& m, uint32_t g0, uint32_t g1, float* rho[2], f
                     int cur, cudaStream_t s);
 void launch_bc_farfield(const DevMesh& m, uint32_t g0, uint32_t g1, float* rho[2], float4* rhou[2],
                         float* rhoe[2], int cur, float3 mach, float p, float t, cudaStream_t s);
-void launch_grad_lim(const DevMesh& m, EulerState q, EulerGrad g, cudaStream_t s);
-void launch_flux(const DevMesh& m, EulerState q, EulerGrad g, float* rho_n, float4* rhou_n, float* rhoe_n,
-                 float* err, double* partials, float cfl, bool transposed, cudaStream_t s);
+void launch_entry_geo(const DevMesh& m, cudaStream_t s);
+void launch_grad_lim(const DevMesh& m, EulerState q, EulerGrad g, bool transposed, cudaStream_t s);
+void launch_flux(const DevMesh& m, EulerState q, FaceRecs r, float* rho_n, float4* rhou_n, float* rhoe_n,
+                 float* err, double* partials, float cfl, cudaStream_t s);
 void launch_reduce_partials(int64_t n, const float* v, double* partials, cudaStream_t s);
 // stage 1 with a caller-chosen number of blocks (one partial per block)
 void launch_reduce_partials_blocks(int64_t n, const float* v, double* partials, int blocks, cudaStream_t s);
