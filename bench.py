@@ -317,6 +317,9 @@ def run_ours(args, rank, world, local_rank):
         batch = run_batch_comparison(args, dev_stream)
     if rank == 0 and world == 1 and not args.skip_warm:
         warm = run_warm_start(args, dev_stream)
+    cyl = None
+    if rank == 0 and world == 1 and not args.skip_cylinder:
+        cyl = run_cylinder(args, dev_stream)
 
     # ---- CPU baseline (rank 0, N = 1) ----
     cpu = None
@@ -346,6 +349,7 @@ def run_ours(args, rank, world, local_rank):
         "time_to_1e-3": ttr,
         "batched_airfoil_sweep": batch,
         "batched_warm_start": warm,
+        "incompressible_cylinder_re40": cyl,
         "cpu_baseline": cpu,
     }
     case.close()
@@ -617,6 +621,55 @@ def run_warm_start(args, dev_stream):
     }
 
 
+def run_cylinder(args, dev_stream):
+    """Config 2: steady incompressible flow past a cylinder at Re = 40 on the
+    400 x 250 O-grid (stretching 1.03, far field at 30 diameters, one cell in
+    span, 100,000 hexes), uniform start, CFL 0.8: iterations and time to the
+    1e-3 drop of the squared residual, then to convergence (1e-10), with the
+    drag coefficient and the closed wake's length at both points."""
+    import torch
+    from graphite_b200 import meshgen
+    from graphite_b200.nsi import NSICase, recirculation_length
+
+    cache = os.path.join(tempfile.gettempdir(), "graphite_b200_bench")
+    os.makedirs(cache, exist_ok=True)
+    path = os.path.join(cache, "cylinder_400x250.su2")
+    if not os.path.exists(path):
+        tmp = path + f".tmp{os.getpid()}"
+        meshgen.cylinder_ogrid(400, 250, ratio=1.03, r_far=30.0).write_su2(tmp)
+        os.replace(tmp, path)
+    bcs = [("wall", "cylinder"), ("inletoutlet", "farfield", 1.0, 0.0, 0.0, 0.0), ("slip", "sides")]
+    NSICase.set_constants(1.0, 1.0 / 40.0, 2.0, True, False)
+    c = NSICase(path)
+    base = c.mesh.contents._cpu.contents
+    cent = np.array([[base.cell_centers[i].x, base.cell_centers[i].y, base.cell_centers[i].z]
+                     for i in range(c.n_cells)])
+    span, out = 0.1, {}
+    for label, tol, check in (("to_1e-3", 1e-3, 1), ("converged_1e-10", 1e-10, 2000)):
+        c.init((1.0, 0.0, 0.0), 0.0)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(dev_stream)
+        h = c.run(bcs, 0.8, 300000, tolerance=tol, check_every=check)
+        e1.record(dev_stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        r = h / h[0]
+        its = int(np.argmax(r < tol)) + 1 if np.any(r < tol) else len(h)
+        f = c.wall_force("cylinder")
+        u, _ = c.fields()
+        out[label] = {"iterations": its, "iterations_run": len(h), "seconds": ms * 1e-3,
+                      "cell_updates_per_s": c.n_cells * len(h) / (ms * 1e-3),
+                      "drag_coefficient": f[0] / (0.5 * span), "lift_coefficient": f[2] / (0.5 * span),
+                      "wake_length_diameters": recirculation_length(cent, u[: c.n_cells]),
+                      "residual_ratio": float(r[-1])}
+    c.close()
+    return {"mesh": "cylinder O-grid 400 x 250 x 1 hexes, stretching 1.03, far field 30 D", "cells": int(base.n_cells),
+            "reynolds": 40, "beta": 2.0, "cfl": 0.8, "laplacian": "average + compact correction",
+            "limiter": "none", **out,
+            "published_range": {"drag_coefficient": [1.50, 1.60], "wake_length_diameters": [2.13, 2.35]}}
+
+
 def run_reference(args, rank, world):
     """The oracle port on the host cores: each step is one bounded sample (a
     block of cells) of the iteration."""
@@ -671,6 +724,7 @@ def main():
     ap.add_argument("--skip-convergence", action="store_true")
     ap.add_argument("--skip-batch", action="store_true", help="skip the batched 64-instance airfoil sweep")
     ap.add_argument("--skip-warm", action="store_true", help="skip the learned warm start (train + evaluate)")
+    ap.add_argument("--skip-cylinder", action="store_true", help="skip the incompressible cylinder (Re 40)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

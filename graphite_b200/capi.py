@@ -104,6 +104,16 @@ _PROTOS = {
     "gbReduceSumNoAlloc": (C.c_int, [C.c_void_p, C.c_uint64, C.c_void_p, C.c_void_p]),
     "gbBatchCreate": (C.c_void_p, [C.c_int, C.POINTER(MeshP), C.c_int, C.POINTER(gbBatchInstance)]),
     "gbBatchSetResidualScale": (C.c_int, [C.c_void_p, C.c_int, C.c_double]),
+    "gbNSISetConstants": (C.c_int, [C.c_float, C.c_float, C.c_float, C.c_int, C.c_int]),
+    "FvmNSIInit": (C.c_int, [MeshP, FieldP, FieldP, gb_vector, C.c_float]),
+    "FvmNSISlipBc": (C.c_int, [MeshP, FieldP, FieldP, C.c_char_p]),
+    "FvmNSIWallBc": (C.c_int, [MeshP, FieldP, FieldP, C.c_char_p]),
+    "FvmNSIInletOutletBc": (C.c_int, [MeshP, FieldP, FieldP, gb_vector, C.c_float, C.c_char_p]),
+    "FvmNSIStepPrepare": (C.c_int, [MeshP, FieldP, FieldP]),
+    "FvmNSIStep": (C.c_int, [MeshP, FieldP, FieldP, C.c_float, C.c_char_p, FieldP, FieldP]),
+    "gbNSIRun": (C.c_int64, [MeshP, FieldP, FieldP, FieldP, C.c_float, C.c_int64, C.POINTER(gbBc), C.c_int,
+                             C.c_double, C.c_int, C.c_void_p]),
+    "gbNSIWallForce": (C.c_int, [MeshP, FieldP, FieldP, C.c_uint, C.c_void_p]),
     "gbWallForce": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint, C.c_void_p]),
     "gbBatchWallForce": (C.c_int, [C.c_void_p, C.c_int, C.c_uint, C.c_void_p]),
     "gbWarmStartCreate": (C.c_void_p, [C.c_void_p, C.c_uint, C.c_uint64]),

@@ -835,3 +835,273 @@ int64_t gbEulerRun(cuMesh* mesh, FvmField* rho, FvmField* rhou, FvmField* rhoe, 
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Incompressible Navier-Stokes by artificial compressibility (nsi.cu).  The
+// reference's src/models/nsi.cu drives FvmNSIInit / FvmNSISlipBc /
+// FvmNSIInletOutletBc / FvmNSIStepPrepare / FvmNSIStep with fields
+// "velocity" (vector) and "pressure" (scalar) but defines none of them; they
+// are defined here with those names and argument meanings, plus a no-slip
+// wall condition, a replayed-graph loop and the wall force.
+namespace gb {
+void launch_nsi_init(int64_t n, float* p, float4* u, float p0, float3 u0, cudaStream_t s);
+void launch_nsi_bc(const DevMesh& m, uint32_t g0, uint32_t g1, int type, float* p[2], float4* u[2], int cur,
+                   float3 vinf, float pinf, cudaStream_t s);
+void launch_nsi_grad(const DevMesh& m, const float* p, const float4* u, float4* gp, float4* gu, int limited,
+                     cudaStream_t s);
+void launch_nsi_flux(const DevMesh& m, const float* p, const float4* u, const float4* gp, const float4* gu, float* p_n,
+                     float4* u_n, float* err, double* partials, float cfl, float nu, float beta2, int corrected,
+                     cudaStream_t s);
+int launch_nsi_force(const DevMesh& m, uint32_t g0, uint32_t g1, const float* p, const float4* u, const float4* gu,
+                     float nu, int corrected, double density, double* partials, double* out, cudaStream_t s);
+
+namespace {
+
+struct NsiConstants {
+    double density = 1.0;
+    double viscosity = 0.025;   // Re = 40 for a unit diameter and unit speed
+    double beta = 2.0;          // artificial sound speed
+    int corrected = 1;
+    int limited = 0;
+};
+thread_local NsiConstants t_nsi;
+
+bool nsi_fields(cuMesh* mesh, FvmField* velocity, FvmField* pressure, const char* what) {
+    if (!check_mesh(mesh)) return false;
+    if (!bind(mesh, velocity, 3, what) || !bind(mesh, pressure, 1, what)) return false;
+    if (impl(velocity)->cur != impl(pressure)->cur) {
+        set_error(std::string(what) + ": velocity and pressure were not updated together");
+        return false;
+    }
+    return true;
+}
+
+bool nsi_grad(cuMesh* mesh, FvmField* f) {
+    FieldImpl* fi = impl(f);
+    if (fi->grad) return true;
+    const int64_t N = impl(mesh)->topo.N;
+    return dalloc(fi->grad, (size_t)N * fi->comps, "alloc gradient") &&
+           cuda_ok(cudaMemsetAsync(fi->grad, 0, (size_t)N * fi->comps * sizeof(float4), t_stream), "zero gradient");
+}
+
+void enqueue_nsi_bc(cuMesh* mesh, FvmField* velocity, FvmField* pressure, int r, int type, int cur, gb_vector v,
+                    float pinf, cudaStream_t s) {
+    MeshImpl* mi = impl(mesh);
+    float* pp[2] = {(float*)impl(pressure)->val[0], (float*)impl(pressure)->val[1]};
+    float4* pu[2] = {(float4*)impl(velocity)->val[0], (float4*)impl(velocity)->val[1]};
+    launch_nsi_bc(mi->dev, mi->num.region_start[r], mi->num.region_start[r + 1], type, pp, pu, cur,
+                  make_float3(v.x, v.y, v.z), pinf, s);
+}
+
+void enqueue_nsi_step(cuMesh* mesh, FvmField* velocity, FvmField* pressure, FvmField* error, float cfl, int cur,
+                      cudaStream_t s) {
+    MeshImpl* mi = impl(mesh);
+    FieldImpl *vi = impl(velocity), *pi = impl(pressure), *ei = impl(error);
+    launch_nsi_grad(mi->dev, (const float*)pi->val[cur], (const float4*)vi->val[cur], pi->grad, vi->grad,
+                    t_nsi.limited, s);
+    launch_nsi_flux(mi->dev, (const float*)pi->val[cur], (const float4*)vi->val[cur], pi->grad, vi->grad,
+                    (float*)pi->val[1 - cur], (float4*)vi->val[1 - cur], (float*)ei->val[ei->cur], ei->partials, cfl,
+                    (float)t_nsi.viscosity, (float)(t_nsi.beta * t_nsi.beta), t_nsi.corrected, s);
+}
+
+int nsi_bc_call(cuMesh* mesh, FvmField* velocity, FvmField* pressure, const char* region, int type, gb_vector v,
+                float p, const char* what) {
+    clear_error();
+    if (!nsi_fields(mesh, velocity, pressure, what)) return 1;
+    const int r = region_lookup(mesh, region);
+    if (r < 0) return 1;
+    enqueue_nsi_bc(mesh, velocity, pressure, r, type, impl(pressure)->cur, v, p, t_stream);
+    return launch_ok(what) ? 0 : 1;
+}
+
+}  // namespace
+}  // namespace gb
+
+extern "C" {
+
+int gbNSISetConstants(gb_scalar density, gb_scalar viscosity, gb_scalar beta, int corrected_laplacian, int limited) {
+    clear_error();
+    if (!(density > 0.f) || !(viscosity >= 0.f) || !(beta > 0.f)) {
+        set_error("gbNSISetConstants: density and beta must be positive, viscosity non-negative");
+        return 1;
+    }
+    t_nsi.density = density;
+    t_nsi.viscosity = viscosity;
+    t_nsi.beta = beta;
+    t_nsi.corrected = corrected_laplacian ? 1 : 0;
+    t_nsi.limited = limited ? 1 : 0;
+    return 0;
+}
+
+int FvmNSIInit(cuMesh* mesh, FvmField* velocity, FvmField* pressure, gb_vector init_velocity, gb_scalar init_pressure) {
+    clear_error();
+    if (!nsi_fields(mesh, velocity, pressure, "FvmNSIInit")) return 1;
+    const int64_t n = (int64_t)impl(pressure)->size;
+    for (int k = 0; k < 2; ++k)
+        launch_nsi_init(n, (float*)impl(pressure)->val[k], (float4*)impl(velocity)->val[k], init_pressure,
+                        make_float3(init_velocity.x, init_velocity.y, init_velocity.z), t_stream);
+    return launch_ok("FvmNSIInit") ? 0 : 1;
+}
+
+int FvmNSISlipBc(cuMesh* mesh, FvmField* velocity, FvmField* pressure, const char* region) {
+    return nsi_bc_call(mesh, velocity, pressure, region, 0, gb_vector{0.f, 0.f, 0.f}, 0.f, "FvmNSISlipBc");
+}
+
+int FvmNSIWallBc(cuMesh* mesh, FvmField* velocity, FvmField* pressure, const char* region) {
+    return nsi_bc_call(mesh, velocity, pressure, region, 2, gb_vector{0.f, 0.f, 0.f}, 0.f, "FvmNSIWallBc");
+}
+
+int FvmNSIInletOutletBc(cuMesh* mesh, FvmField* velocity, FvmField* pressure, gb_vector inlet_velocity,
+                        gb_scalar outlet_pressure, const char* region) {
+    return nsi_bc_call(mesh, velocity, pressure, region, 1, inlet_velocity, outlet_pressure, "FvmNSIInletOutletBc");
+}
+
+int FvmNSIStepPrepare(cuMesh* mesh, FvmField* velocity, FvmField* pressure) {
+    clear_error();
+    if (!nsi_fields(mesh, velocity, pressure, "FvmNSIStepPrepare")) return 1;
+    if (!nsi_grad(mesh, velocity) || !nsi_grad(mesh, pressure)) return 1;
+    const int cur = impl(pressure)->cur;
+    launch_nsi_grad(impl(mesh)->dev, (const float*)impl(pressure)->val[cur], (const float4*)impl(velocity)->val[cur],
+                    impl(pressure)->grad, impl(velocity)->grad, t_nsi.limited, t_stream);
+    return launch_ok("FvmNSIStepPrepare") ? 0 : 1;
+}
+
+int FvmNSIStep(cuMesh* mesh, FvmField* velocity, FvmField* pressure, gb_scalar cfl, const char* time_scheme,
+               FvmField* dt, FvmField* error) {
+    (void)dt;
+    clear_error();
+    if (!time_scheme || strcmp(time_scheme, "steady") != 0) {
+        set_error("FvmNSIStep: only the \"steady\" scheme exists");
+        return 1;
+    }
+    if (!nsi_fields(mesh, velocity, pressure, "FvmNSIStep") || !bind(mesh, error, 1, "FvmNSIStep")) return 1;
+    if (!impl(velocity)->grad || !impl(pressure)->grad) {
+        set_error("FvmNSIStep: call FvmNSIStepPrepare first");
+        return 1;
+    }
+    MeshImpl* mi = impl(mesh);
+    FieldImpl* ei = impl(error);
+    const int nb = (int)((mi->dev.N + kBlock - 1) / kBlock);
+    if (!ensure_partials(ei, std::max(nb, 1))) return 1;
+    const int cur = impl(pressure)->cur;
+    FieldImpl *vi = impl(velocity), *pi = impl(pressure);
+    launch_nsi_flux(mi->dev, (const float*)pi->val[cur], (const float4*)vi->val[cur], pi->grad, vi->grad,
+                    (float*)pi->val[1 - cur], (float4*)vi->val[1 - cur], (float*)ei->val[ei->cur], ei->partials, cfl,
+                    (float)t_nsi.viscosity, (float)(t_nsi.beta * t_nsi.beta), t_nsi.corrected, t_stream);
+    if (!launch_ok("FvmNSIStep")) return 1;
+    vi->cur = pi->cur = 1 - cur;
+    ei->partials_valid = true;
+    return 0;
+}
+
+int64_t gbNSIRun(cuMesh* mesh, FvmField* velocity, FvmField* pressure, FvmField* error, gb_scalar cfl, int64_t n_iter,
+                 const gbBc* bcs, int n_bc, double tolerance, int check_every, double* residual_history) {
+    clear_error();
+    if (n_iter < 0 || n_bc < 0 || (n_bc > 0 && !bcs)) { set_error("gbNSIRun: bad arguments"); return -1; }
+    if (!nsi_fields(mesh, velocity, pressure, "gbNSIRun") || !bind(mesh, error, 1, "gbNSIRun")) return -1;
+    MeshImpl* mi = impl(mesh);
+    for (int b = 0; b < n_bc; ++b)
+        if (bcs[b].region_id >= mi->topo.regions.size() || bcs[b].type < 0 || bcs[b].type > 2) {
+            set_error("gbNSIRun: bad boundary condition " + std::to_string(b));
+            return -1;
+        }
+    if (n_iter == 0) return 0;
+    if (!nsi_grad(mesh, velocity) || !nsi_grad(mesh, pressure)) return -1;
+    FieldImpl* ei = impl(error);
+    const int nb = (int)((mi->dev.N + kBlock - 1) / kBlock);
+    if (!ensure_partials(ei, std::max(nb, 1))) return -1;
+    if (check_every <= 0) check_every = 100;
+    cudaStream_t s = t_stream;
+    double* d_hist = nullptr;
+    unsigned long long* d_counter = nullptr;
+    if (!dalloc(d_hist, (size_t)n_iter, "gbNSIRun") || !dalloc(d_counter, 1, "gbNSIRun") ||
+        !cuda_ok(cudaMemsetAsync(d_counter, 0, sizeof(unsigned long long), s), "gbNSIRun")) {
+        dfree(d_hist); dfree(d_counter);
+        return -1;
+    }
+    double* out = mi->dev.red + mi->dev.n_red_max;
+    cudaGraphExec_t exec[2] = {nullptr, nullptr};
+    cudaStream_t cap = nullptr;
+    bool ok = cuda_ok(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking), "gbNSIRun");
+    t_counting = false;
+    for (int k = 0; k < 2 && ok; ++k) {
+        cudaGraph_t g = nullptr;
+        ok = cuda_ok(cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal), "graph capture");
+        if (!ok) break;
+        for (int b = 0; b < n_bc; ++b) {
+            const int type = bcs[b].type == 1 ? 1 : (bcs[b].type == 2 ? 2 : 0);
+            enqueue_nsi_bc(mesh, velocity, pressure, (int)bcs[b].region_id, type, k, bcs[b].mach, bcs[b].pressure, cap);
+        }
+        enqueue_nsi_step(mesh, velocity, pressure, error, cfl, k, cap);
+        launch_reduce_final(nb, ei->partials, out, d_hist, d_counter, cap);
+        ok = cuda_ok(cudaStreamEndCapture(cap, &g), "graph capture") &&
+             cuda_ok(cudaGraphInstantiate(&exec[k], g, 0), "graph instantiate");
+        if (g) cudaGraphDestroy(g);
+    }
+    t_counting = true;
+    const int per_iter = n_bc + 3;
+    int cur = impl(pressure)->cur;
+    int64_t done = 0;
+    std::vector<double> hist((size_t)n_iter, 0.0);
+    while (ok && done < n_iter) {
+        const int64_t chunk = std::min<int64_t>(check_every, n_iter - done);
+        for (int64_t i = 0; i < chunk && ok; ++i) {
+            ok = cuda_ok(cudaGraphLaunch(exec[cur], s), "graph launch");
+            count_launch(per_iter);
+            cur = 1 - cur;
+        }
+        done += chunk;
+        if (!ok) break;
+        ok = cuda_ok(cudaMemcpyAsync(hist.data(), d_hist, done * sizeof(double), cudaMemcpyDeviceToHost, s), "gbNSIRun") &&
+             cuda_ok(cudaStreamSynchronize(s), "gbNSIRun");
+        if (ok && tolerance > 0.0 && hist[0] > 0.0) {
+            bool stop = false;
+            for (int64_t i = done - chunk; i < done && !stop; ++i) stop = hist[i] / hist[0] < tolerance;
+            if (stop) break;
+        }
+        if (ok) {
+            bool bad = false;
+            for (int64_t i = done - chunk; i < done; ++i) bad |= !std::isfinite(hist[i]);
+            if (bad) { set_error("gbNSIRun: residual is not finite (diverged)"); ok = false; }
+        }
+    }
+    impl(velocity)->cur = impl(pressure)->cur = cur;
+    ei->partials_valid = true;
+    if (residual_history) memcpy(residual_history, hist.data(), (size_t)done * sizeof(double));
+    for (int k = 0; k < 2; ++k) if (exec[k]) cudaGraphExecDestroy(exec[k]);
+    if (cap) cudaStreamDestroy(cap);
+    dfree(d_hist);
+    dfree(d_counter);
+    return ok ? done : -1;
+}
+
+int gbNSIWallForce(cuMesh* mesh, FvmField* velocity, FvmField* pressure, unsigned region_id, double* force) {
+    clear_error();
+    if (!force) { set_error("gbNSIWallForce: null output"); return 1; }
+    if (!nsi_fields(mesh, velocity, pressure, "gbNSIWallForce")) return 1;
+    MeshImpl* mi = impl(mesh);
+    if (region_id >= mi->topo.regions.size()) { set_error("gbNSIWallForce: unknown region"); return 1; }
+    if (!impl(velocity)->grad) { set_error("gbNSIWallForce: call FvmNSIStepPrepare or gbNSIRun first"); return 1; }
+    const uint32_t g0 = mi->num.region_start[region_id], g1 = mi->num.region_start[region_id + 1];
+    force[0] = force[1] = force[2] = 0.0;
+    if (g1 <= g0) return 0;
+    const int blocks = (int)((g1 - g0 + kBlock - 1) / kBlock);
+    double* d = nullptr;
+    if (!dalloc(d, (size_t)3 * blocks + 3, "gbNSIWallForce")) return 1;
+    const int cur = impl(pressure)->cur;
+    cudaStream_t s = t_stream;
+    // the gradient of the current state (the one stored may be a step old)
+    launch_nsi_grad(mi->dev, (const float*)impl(pressure)->val[cur], (const float4*)impl(velocity)->val[cur],
+                    impl(pressure)->grad, impl(velocity)->grad, t_nsi.limited, s);
+    launch_nsi_force(mi->dev, g0, g1, (const float*)impl(pressure)->val[cur], (const float4*)impl(velocity)->val[cur],
+                     impl(velocity)->grad, (float)t_nsi.viscosity, t_nsi.corrected, t_nsi.density, d, d + 3 * blocks,
+                     s);
+    const bool ok = launch_ok("gbNSIWallForce") &&
+                    cuda_ok(cudaMemcpyAsync(force, d + 3 * blocks, 3 * sizeof(double), cudaMemcpyDeviceToHost, s),
+                            "gbNSIWallForce") &&
+                    cuda_ok(cudaStreamSynchronize(s), "gbNSIWallForce");
+    dfree(d);
+    return ok ? 0 : 1;
+}
+
+}  // extern "C"

@@ -365,6 +365,46 @@ int gbWarmStartForward(gbWarmStart* ws, int64_t n, const float* x, float* y);
 int gbWallForce(cuMesh* mesh, FvmField* rho, FvmField* rhou, FvmField* rhoe, unsigned region_id, double* force);
 int gbBatchWallForce(gbBatch* batch, int instance, unsigned region_id, double* force);
 
+/* ---- Incompressible Navier-Stokes (artificial compressibility) ----
+ * The reference's NSI model (src/models/nsi.cu:71,114,137,144) calls
+ * FvmNSIInit, FvmNSISlipBc, FvmNSIInletOutletBc, FvmNSIStepPrepare and
+ * FvmNSIStep on a "velocity" (vector) and a "pressure" (scalar, p / rho)
+ * field but never defines them; these are those calls.  Steady solutions of
+ * div u = 0, div(u u + p I) = nu lap u are reached in pseudo-time
+ * (dp/dt + beta^2 div u = 0) with second-order LSQ reconstruction, the
+ * reference's limiter, a Rusanov flux with the artificial-compressibility
+ * wave speed, and local time steps.  Constants (per thread, like the stream):
+ * density (scales forces), kinematic viscosity nu, artificial sound speed
+ * beta, and the face gradient of the viscous term: the two cells' average as
+ * fvmLaplacianC (include/fvmops.cuh:96-102) takes it (0), or that average
+ * with the compact correction along the centroid offset (1, default), and
+ * whether the reconstruction uses the reference's limiter (1) or none (0,
+ * default: smooth incompressible flow needs none, and the limiter's first-
+ * order switching adds dissipation that shortens a laminar wake). */
+int gbNSISetConstants(gb_scalar density, gb_scalar viscosity, gb_scalar beta, int corrected_laplacian, int limited);
+int FvmNSIInit(cuMesh* mesh, FvmField* velocity, FvmField* pressure, gb_vector init_velocity, gb_scalar init_pressure);
+/* symmetry: normal velocity mirrored, pressure extrapolated */
+int FvmNSISlipBc(cuMesh* mesh, FvmField* velocity, FvmField* pressure, const char* region);
+/* no-slip wall: velocity mirrored through zero, pressure extrapolated (new) */
+int FvmNSIWallBc(cuMesh* mesh, FvmField* velocity, FvmField* pressure, const char* region);
+/* inflow (inlet_velocity . n < 0): that velocity, interior pressure;
+ * outflow: interior velocity, outlet_pressure */
+int FvmNSIInletOutletBc(cuMesh* mesh, FvmField* velocity, FvmField* pressure, gb_vector inlet_velocity,
+                        gb_scalar outlet_pressure, const char* region);
+int FvmNSIStepPrepare(cuMesh* mesh, FvmField* velocity, FvmField* pressure);
+/* error[i] = (R_p^2 + |R_u|^2) V, summed by FvmFieldReduceSum */
+int FvmNSIStep(cuMesh* mesh, FvmField* velocity, FvmField* pressure, gb_scalar cfl, const char* time_scheme,
+               FvmField* dt, FvmField* error);
+/* The whole loop as replayed graphs (as gbEulerRun).  Boundary conditions:
+ * type 0 slip, 1 inlet / outlet (mach = inlet velocity, pressure = outlet
+ * pressure), 2 no-slip wall. */
+int64_t gbNSIRun(cuMesh* mesh, FvmField* velocity, FvmField* pressure, FvmField* error, gb_scalar cfl,
+                 int64_t n_iter, const gbBc* bcs, int n_bc, double tolerance, int check_every,
+                 double* residual_history);
+/* Force on a wall region: density * sum of A (p n - nu (grad u)_f . n), n out
+ * of the fluid; float64, deterministic. */
+int gbNSIWallForce(cuMesh* mesh, FvmField* velocity, FvmField* pressure, unsigned region_id, double* force);
+
 /* Sum of n float values in device memory into *result (one double in device
  * memory), accumulated in float64 in a fixed order: the reduction behind
  * FvmFieldReduceSum, for callers that cannot allocate device memory -- code
