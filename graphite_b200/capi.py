@@ -104,6 +104,8 @@ _PROTOS = {
     "gbReduceSumNoAlloc": (C.c_int, [C.c_void_p, C.c_uint64, C.c_void_p, C.c_void_p]),
     "gbBatchCreate": (C.c_void_p, [C.c_int, C.POINTER(MeshP), C.c_int, C.POINTER(gbBatchInstance)]),
     "gbBatchSetResidualScale": (C.c_int, [C.c_void_p, C.c_int, C.c_double]),
+    "FieldsWriteVtu": (C.c_int, [C.c_char_p, MeshP, C.POINTER(FieldP), C.c_size_t]),
+    "gbFieldsWriteVtuBinary": (C.c_int, [C.c_char_p, MeshP, C.POINTER(FieldP), C.c_size_t]),
     "gbNSISetConstants": (C.c_int, [C.c_float, C.c_float, C.c_float, C.c_int, C.c_int]),
     "FvmNSIInit": (C.c_int, [MeshP, FieldP, FieldP, gb_vector, C.c_float]),
     "FvmNSISlipBc": (C.c_int, [MeshP, FieldP, FieldP, C.c_char_p]),

@@ -365,6 +365,14 @@ int gbWarmStartForward(gbWarmStart* ws, int64_t n, const float* x, float* y);
 int gbWallForce(cuMesh* mesh, FvmField* rho, FvmField* rhou, FvmField* rhoe, unsigned region_id, double* force);
 int gbBatchWallForce(gbBatch* batch, int instance, unsigned region_id, double* force);
 
+/* Writes the mesh (VTK polyhedra, type 42) and the fields' host values (one
+ * per interior cell; call VarGpuToCpu first) as an ASCII VTU file, as the
+ * reference's FieldsWriteVtu (src/fvmfieldsio.cu:5-287; include/
+ * fvmfieldsio.cuh:12-17) does.  gbFieldsWriteVtuBinary writes the same file
+ * with raw appended binary arrays.  0 on success. */
+int FieldsWriteVtu(const char* filename, cuMesh* mesh, const FvmField** vars, const size_t nvars);
+int gbFieldsWriteVtuBinary(const char* filename, cuMesh* mesh, const FvmField** vars, const size_t nvars);
+
 /* ---- Incompressible Navier-Stokes (artificial compressibility) ----
  * The reference's NSI model (src/models/nsi.cu:71,114,137,144) calls
  * FvmNSIInit, FvmNSISlipBc, FvmNSIInletOutletBc, FvmNSIStepPrepare and
