@@ -104,6 +104,9 @@ _PROTOS = {
     "gbReduceSumNoAlloc": (C.c_int, [C.c_void_p, C.c_uint64, C.c_void_p, C.c_void_p]),
     "gbBatchCreate": (C.c_void_p, [C.c_int, C.POINTER(MeshP), C.c_int, C.POINTER(gbBatchInstance)]),
     "gbBatchSetResidualScale": (C.c_int, [C.c_void_p, C.c_int, C.c_double]),
+    "gbFvmGradient": (C.c_int, [MeshP, FieldP]),
+    "gbFvmApply": (C.c_int, [MeshP, C.c_int, FieldP, FieldP, gb_vector, C.c_void_p]),
+    "gbRenderRegionScalar": (C.c_int64, [MeshP, C.c_uint, FieldP, C.c_float, C.c_float, C.c_void_p, C.c_int64]),
     "FieldsWriteVtu": (C.c_int, [C.c_char_p, MeshP, C.POINTER(FieldP), C.c_size_t]),
     "gbFieldsWriteVtuBinary": (C.c_int, [C.c_char_p, MeshP, C.POINTER(FieldP), C.c_size_t]),
     "gbNSISetConstants": (C.c_int, [C.c_float, C.c_float, C.c_float, C.c_int, C.c_int]),

@@ -464,6 +464,7 @@ bool field_access(FvmField* f, cuMesh* mesh, int comps, FieldAccess* out) {
     out->cur = fi->cur;
     out->comps = fi->comps;
     out->size = fi->size;
+    out->grad = fi->grad;
     return true;
 }
 
@@ -1102,6 +1103,70 @@ int gbNSIWallForce(cuMesh* mesh, FvmField* velocity, FvmField* pressure, unsigne
                     cuda_ok(cudaStreamSynchronize(s), "gbNSIWallForce");
     dfree(d);
     return ok ? 0 : 1;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Generic finite-volume operators (fvmops.cu).
+namespace gb {
+void launch_fvm_grad(const DevMesh& m, int comps, const float* s, const float4* v, float4* grad, cudaStream_t st);
+void launch_fvm_apply(const DevMesh& m, int op, const float* s, const float4* v, const float4* g, const float4* phi,
+                      float3 phi_c, float* out, cudaStream_t st);
+}  // namespace gb
+
+extern "C" {
+
+int gbFvmGradient(cuMesh* mesh, FvmField* u) {
+    clear_error();
+    if (!check_mesh(mesh)) return 1;
+    FieldImpl* fi = impl(u);
+    if (!fi || !bind(mesh, u, fi->comps, "gbFvmGradient") || !nsi_grad(mesh, u)) return 1;
+    launch_fvm_grad(impl(mesh)->dev, fi->comps, fi->comps == 1 ? (const float*)fi->val[fi->cur] : nullptr,
+                    fi->comps == 3 ? (const float4*)fi->val[fi->cur] : nullptr, fi->grad, t_stream);
+    return launch_ok("gbFvmGradient") ? 0 : 1;
+}
+
+int gbFvmApply(cuMesh* mesh, int op, FvmField* u, FvmField* phi, gb_vector phi_const, float* out) {
+    clear_error();
+    if (!check_mesh(mesh) || !out) { if (!out) set_error("gbFvmApply: null output"); return 1; }
+    FieldImpl* fi = impl(u);
+    if (!fi) { set_error("gbFvmApply: null field"); return 1; }
+    static const int in_comps[11] = {1, 1, 1, 3, 1, 3, 3, 1, 1, 1, 3};
+    static const int out_comps[11] = {1, 3, 3, 9, 3, 9, 1, 1, 1, 1, 3};
+    static const bool needs_grad[11] = {true, false, true, false, false, false, false, false, true, false, false};
+    if (op < 0 || op > 10) { set_error("gbFvmApply: unknown operator"); return 1; }
+    if (!bind(mesh, u, in_comps[op], "gbFvmApply")) return 1;
+    if (needs_grad[op] && !fi->grad) { set_error("gbFvmApply: the operator needs the field's gradient (gbFvmGradient)"); return 1; }
+    const float4* phi_v = nullptr;
+    if (op == 9 || op == 10) {
+        if (!phi || !bind(mesh, phi, 3, "gbFvmApply")) { if (!phi) set_error("gbFvmApply: the operator needs a vector field phi"); return 1; }
+        phi_v = (const float4*)impl(phi)->val[impl(phi)->cur];
+    }
+    MeshImpl* mi = impl(mesh);
+    const int64_t N = mi->dev.N;
+    const int oc = out_comps[op];
+    float *d_out = nullptr, *d_ref = nullptr;
+    if (!dalloc(d_out, (size_t)oc * N, "gbFvmApply") || !dalloc(d_ref, (size_t)oc * N, "gbFvmApply")) {
+        dfree(d_out); dfree(d_ref);
+        return 1;
+    }
+    cudaStream_t s = t_stream;
+    launch_fvm_apply(mi->dev, op, fi->comps == 1 ? (const float*)fi->val[fi->cur] : nullptr,
+                     fi->comps == 3 ? (const float4*)fi->val[fi->cur] : nullptr, fi->grad, phi_v,
+                     make_float3(phi_const.x, phi_const.y, phi_const.z), d_out, s);
+    for (int q = 0; q < oc; ++q) launch_gather_scalar(N, d_out + (size_t)q * N, mi->d_cell_new, d_ref + (size_t)q * N, s);
+    std::vector<float> h((size_t)oc * N);
+    const bool ok = launch_ok("gbFvmApply") &&
+                    cuda_ok(cudaMemcpyAsync(h.data(), d_ref, h.size() * sizeof(float), cudaMemcpyDeviceToHost, s),
+                            "gbFvmApply") &&
+                    cuda_ok(cudaStreamSynchronize(s), "gbFvmApply");
+    dfree(d_out);
+    dfree(d_ref);
+    if (!ok) return 1;
+    for (int64_t i = 0; i < N; ++i)
+        for (int q = 0; q < oc; ++q) out[i * oc + q] = h[(size_t)q * N + i];
+    return 0;
 }
 
 }  // extern "C"

@@ -142,6 +142,7 @@ struct FieldAccess {
     int cur;
     int comps;                             // 1 scalar (float), 3 vector (float4)
     size_t size;
+    const float4* grad;                    // last stored gradients + limiters, or null
 };
 // Binds the field to `mesh` (its device order becomes the mesh's) and checks
 // its size and number of components.

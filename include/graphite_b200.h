@@ -373,6 +373,41 @@ int gbBatchWallForce(gbBatch* batch, int instance, unsigned region_id, double* f
 int FieldsWriteVtu(const char* filename, cuMesh* mesh, const FvmField** vars, const size_t nvars);
 int gbFieldsWriteVtuBinary(const char* filename, cuMesh* mesh, const FvmField** vars, const size_t nvars);
 
+/* Headless colour map of a scalar field on a boundary region: what the
+ * reference's renderer writes into its OpenGL buffer (RenderMesh from a
+ * region, src/render/window.cu:560-627; KernelRenderScalarField, :682-756),
+ * written to `out` (host or device memory): 18 floats per triangle,
+ * (x, y, z, r, g, b) for each of its 3 vertices.  Colours use the field's
+ * last stored gradients and limiters (FvmEulerStepPrepare; zero before the
+ * first).  out = NULL returns the number of triangles; otherwise returns
+ * the number written, or -1 (also if capacity_triangles is too small). */
+int64_t gbRenderRegionScalar(cuMesh* mesh, unsigned region_id, FvmField* field, gb_scalar u_min, gb_scalar u_max,
+                             float* out, int64_t capacity_triangles);
+
+/* ---- Generic finite-volume operators (include/fvmops.cuh:96-219) ----
+ * gbFvmGradient: least-squares gradient and limiter of any scalar or vector
+ * field (ScalarVarComputeGradient / VectorVarComputeGradient and the limiter
+ * pass, src/fvmops.cu:51-266), stored in the field (VarAllGpuToCpu shows
+ * them); a ghost carries its interior cell's.
+ * gbFvmApply: one operator over every interior cell, out[n_cells x k] in the
+ * reference's cell order, k = 1 (scalar), 3 (vector) or 9 (tensor
+ * {u, v, w}, outer(a, b) = (a b.x, a b.y, a b.z)). */
+enum {
+    GB_FVM_LAPLACIAN = 0,          /* fvmLaplacianC       scalar -> scalar, needs gradient */
+    GB_FVM_SCAL_GRAD = 1,          /* fvmScalGradC        scalar -> vector */
+    GB_FVM_SCAL_GRAD_CORRECT = 2,  /* fvmScalGradCCorrect scalar -> vector, needs gradient */
+    GB_FVM_VEC_GRAD = 3,           /* fvmVecGradC         vector -> tensor */
+    GB_FVM_BOUND_SCAL_GRAD = 4,    /* fvmBoundScalGradC   scalar -> vector */
+    GB_FVM_BOUND_VEC_GRAD = 5,     /* fvmBoundVecGradC    vector -> tensor */
+    GB_FVM_DIV = 6,                /* fvmDivC             vector -> scalar */
+    GB_FVM_CONV_CONST_SCAL = 7,    /* fvmConvConstScalU   scalar, constant phi -> scalar */
+    GB_FVM_CONV_CONST_SCAL2 = 8,   /* fvmConvConstScalU2  scalar, constant phi -> scalar, needs gradient */
+    GB_FVM_CONV_SCAL = 9,          /* fvmConvScalU        scalar, vector field phi -> scalar */
+    GB_FVM_CONV_VEC = 10           /* fvmConvVecU         vector, vector field phi -> vector */
+};
+int gbFvmGradient(cuMesh* mesh, FvmField* u);
+int gbFvmApply(cuMesh* mesh, int op, FvmField* u, FvmField* phi, gb_vector phi_const, float* out);
+
 /* ---- Incompressible Navier-Stokes (artificial compressibility) ----
  * The reference's NSI model (src/models/nsi.cu:71,114,137,144) calls
  * FvmNSIInit, FvmNSISlipBc, FvmNSIInletOutletBc, FvmNSIStepPrepare and

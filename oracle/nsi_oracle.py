@@ -32,8 +32,8 @@ def limiter(u, g, umin, umax, d, k3):
         sig = np.where(dmm2 <= k3, 1.0, np.where(dmm2 <= 2.0 * k3, 2 * y ** 3 - 3 * y ** 2 + 1.0, 0.0))
         yp = du / delta
         yn = dd / delta
-    lp = np.where(yp < 2.0, yp - 0.25 * yp * yp, 1.0)
-    ln = np.where(yn < 2.0, yn - 0.25 * yn * yn, 1.0)
+        lp = np.where(yp < 2.0, yp - 0.25 * yp * yp, 1.0)
+        ln = np.where(yn < 2.0, yn - 0.25 * yn * yn, 1.0)
     lim = np.where(delta > 1e-6, lp, np.where(delta < -1e-6, ln, 1.0)) * 0.8
     return sig + (1.0 - sig) * lim
 

@@ -1,0 +1,65 @@
+"""The generic finite-volume operators (gbFvmApply) and field gradients
+(gbFvmGradient) against their FP64 restatement."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+import cases
+from graphite_b200 import capi
+from oracle.fvmops_oracle import OpMesh
+from oracle.pyoracle import OracleMesh
+
+pytestmark = pytest.mark.gpu
+
+OUT = {0: 1, 1: 3, 2: 3, 3: 9, 4: 3, 5: 9, 6: 1, 7: 1, 8: 1, 9: 1, 10: 3}
+
+
+def _field(lib, mesh, n, comps, name, values):
+    f = lib.FvmFieldNew(4 * comps, n, name, 1)
+    capi.set_field_values(f, values)
+    capi.check(lib.gbVarCpuToGpu(mesh, f), "gbVarCpuToGpu")
+    return f
+
+
+@pytest.mark.parametrize("name", ["tet_6x3x2", "prism_6x3x2", "hex_6x3x2"])
+def test_operators_match_restatement(su2_paths, workdir, name):
+    lib = capi.load()
+    em = cases.MESHES[name]()
+    fvm = str(workdir / f"{name}_ops.fvm")
+    capi.check(lib.cuMeshFromSu2(su2_paths(name).encode(), fvm.encode()), "cuMeshFromSu2")
+    mesh = lib.cuMeshFromFile(fvm.encode())
+    n = int(lib.cuMeshGetVarSize(mesh))
+    base = mesh.contents._cpu.contents
+    x = np.array([[base.cell_centers[i].x, base.cell_centers[i].y, base.cell_centers[i].z] for i in range(n)])
+    rng = np.random.default_rng(4)
+    s = (np.sin(2 * x[:, 0]) + x[:, 1] ** 2 + 0.05 * rng.standard_normal(n)).astype(np.float32)
+    v = np.column_stack([np.cos(x[:, 1]), x[:, 0] * x[:, 2], 1 + 0.1 * rng.standard_normal(n)]).astype(np.float32)
+    ph = np.column_stack([1 + 0.2 * x[:, 1], 0.3 * np.ones(n), -0.2 + 0.1 * x[:, 0]]).astype(np.float32)
+    fs, fv, fp = _field(lib, mesh, n, 1, b"s", s), _field(lib, mesh, n, 3, b"v", v), _field(lib, mesh, n, 3, b"phi", ph)
+    om = OpMesh(OracleMesh(em))
+    N = om.N
+    # gradients of the scalar and the vector field
+    for f, vals, k in ((fs, s, 1), (fv, v, 3)):
+        capi.check(lib.gbFvmGradient(mesh, f), "gbFvmGradient")
+        lib.VarAllGpuToCpu(f)
+        g, l = capi.field_gradients(f)
+        gr, lr = om.gradient(vals.astype(np.float64))
+        g = g[:N].reshape(N, k, 3)         # host mirror: [cell][component][x, y, z]
+        np.testing.assert_allclose(g, gr, atol=2e-5 * np.max(np.abs(gr)))
+        np.testing.assert_allclose(np.asarray(l[:N]).reshape(N, k), lr, atol=2e-4)
+    gs, ls = om.gradient(s.astype(np.float64))
+    phi_c = (0.7, -0.2, 0.4)
+    for op, k in OUT.items():
+        u = fv if op in (3, 5, 6, 10) else fs
+        out = np.zeros((N, k), np.float32)
+        capi.check(lib.gbFvmApply(mesh, op, u, fp, capi.vec(phi_c), out.ctypes.data), f"gbFvmApply {op}")
+        uu = (v if op in (3, 5, 6, 10) else s).astype(np.float64)
+        ref = om.apply(op, uu, grad=gs, lim=ls, phi=ph.astype(np.float64), phi_c=phi_c).reshape(N, k)
+        scale = max(np.max(np.abs(ref)), 1e-12)
+        assert np.max(np.abs(out - ref)) <= 2e-5 * scale + 1e-6, (op, np.max(np.abs(out - ref)) / scale)
+    assert lib.gbFvmApply(mesh, 3, fs, None, capi.vec(phi_c), out.ctypes.data) != 0     # tensor op on a scalar
+    assert lib.gbFvmApply(mesh, 11, fs, None, capi.vec(phi_c), out.ctypes.data) != 0
+    for f in (fs, fv, fp):
+        lib.FvmFieldFree(f)
+    lib.cuMeshFree(mesh)
