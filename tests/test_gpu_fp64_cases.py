@@ -1,0 +1,65 @@
+"""The FP32 solver against an FP64 oracle run of the same scheme on the
+benchmark meshes: the transonic swept wing (1.1 M prisms) and the 120k
+airfoil, each from free stream to the 1e-3 drop of the squared residual.
+States the density L2 error and the lift/drag errors."""
+import math
+
+import numpy as np
+import pytest
+
+import cases
+from graphite_b200 import capi, meshgen
+from graphite_b200.euler import EulerCase
+from oracle import pyoracle
+
+pytestmark = pytest.mark.gpu
+
+
+def _compare(em, path, bcs, mach, cfl, wall):
+    capi.load().gbSetReferenceMomentumReconstruction(1)
+    c = EulerCase(path)
+    c.init(mach, cases.P_INF, cases.T_INF)
+    h = c.run(bcs, cfl, 20000, tolerance=1e-3, check_every=1)
+    n_it = len(h)
+    f32 = c.wall_force(wall)
+    rho32 = c.fields()[0]
+    N = c.n_cells
+    c.close()
+    om = pyoracle.OracleMesh(em)
+    s = pyoracle.OracleSolver(om, bits=64)
+    s.init(mach, cases.P_INF, cases.T_INF)
+    h64 = s.run(bcs, n_it, cfl)
+    f64 = pyoracle.wall_force(om, s.get("rho"), s.get("rhou"), s.get("rhoe"), wall)
+    l32, d32 = pyoracle.lift_drag(f32, mach)
+    l64, d64 = pyoracle.lift_drag(f64, mach)
+    rho64 = s.get("rho")
+    l2 = np.linalg.norm(rho32[:N] - rho64[:N]) / np.linalg.norm(rho64[:N])
+    return n_it, h64[-1] / h64[0], l2, abs(l32 - l64) / abs(l64), abs(d32 - d64) / abs(d64), (l32, l64, d32, d64)
+
+
+def test_swept_wing_to_1e3_against_fp64(workdir):
+    em = meshgen.swept_wing()
+    path = str(workdir / "wing_fp64.su2")
+    em.write_su2(path)
+    a = math.radians(3.0)
+    mach = (0.84 * math.cos(a), 0.0, 0.84 * math.sin(a))
+    bcs = [("farfield", "farfield") + mach + (cases.P_INF, cases.T_INF), ("slip", "symmetry"), ("slip", "wing")]
+    n_it, r64, l2, el, ed, v = _compare(em, path, bcs, mach, 0.8, "wing")
+    print(f"swept wing, {n_it} iterations: FP64 residual ratio {r64:.3e}, rho L2 {l2:.2e}, "
+          f"lift {v[0]:.6e} vs {v[1]:.6e} ({el:.2e}), drag {v[2]:.6e} vs {v[3]:.6e} ({ed:.2e})")
+    assert r64 < 1.2e-3
+    assert l2 < 2e-4 and el < 2e-3 and ed < 1e-2
+
+
+def test_airfoil_120k_to_1e3_against_fp64(workdir):
+    em = meshgen.airfoil_extruded(120_000)
+    path = str(workdir / "airfoil120k_fp64.su2")
+    em.write_su2(path)
+    a = math.radians(2.5)
+    mach = (0.6 * math.cos(a), 0.0, 0.6 * math.sin(a))
+    bcs = [("farfield", "farfield") + mach + (cases.P_INF, cases.T_INF), ("slip", "sides"), ("slip", "wing")]
+    n_it, r64, l2, el, ed, v = _compare(em, path, bcs, mach, 0.5, "wing")
+    print(f"airfoil 120k, {n_it} iterations: FP64 residual ratio {r64:.3e}, rho L2 {l2:.2e}, "
+          f"lift {v[0]:.6e} vs {v[1]:.6e} ({el:.2e}), drag {v[2]:.6e} vs {v[3]:.6e} ({ed:.2e})")
+    assert r64 < 1.5e-3
+    assert l2 < 1e-4 and el < 2e-3 and ed < 2e-2
