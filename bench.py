@@ -710,6 +710,7 @@ def run_reference(args, rank, world):
         c = 0 if c1 >= N else c1
     dt = time.perf_counter() - t0
     v = done / dt
+    ref_gpu = reference_gpu_build(args.workload)
     return {"metric": "cell-updates/s", "value": v, "unit": "cell-updates/s", "impl": "reference",
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3 / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
@@ -720,7 +721,46 @@ def run_reference(args, rank, world):
                              "sample": f"{args.steps} blocks of {block} cells (one block per step)"},
             "e2e": {"value": v, "unit": "cell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
             "note": "the reference has no host implementation of this path (all of it is CUDA); this is the "
-                    "oracle, a C++ restatement of the reference's kernels, with OpenMP over cells"}
+                    "oracle, a C++ restatement of the reference's kernels, with OpenMP over cells",
+            "reference_gpu_build": ref_gpu}
+
+
+def reference_gpu_build(workload, iters=300):
+    """The reference's own CUDA build (its solver sources compiled headless,
+    oracle/_ref/ref_driver) on the same mesh and case, on this GPU: its
+    PhysicsEuler loop (BCs, FvmEulerStepPrepare, FvmEulerStep,
+    FvmFieldReduceSum with the whole error field copied to the host) for
+    `iters` iterations, as the binary reports it.  None where the build or a
+    GPU is absent."""
+    exe = os.path.join(ROOT, "oracle", "_ref", "ref_driver")
+    try:
+        import torch
+        if not (os.path.exists(exe) and torch.cuda.is_available()):
+            return None
+    except Exception:
+        return None
+    cache = os.path.join(tempfile.gettempdir(), "graphite_b200_bench")
+    os.makedirs(cache, exist_ok=True)
+    su2, bcs, mach = mesh_file(workload, cache)
+    case = os.path.join(cache, f"{workload}_ref_case.txt")
+    with open(case, "w") as f:
+        f.write(f"init {mach[0]} {mach[1]} {mach[2]} {P_INF} {T_INF}\n")
+        for b in bcs:
+            f.write(f"slip {b[1]}\n" if b[0] == "slip" else f"farfield {b[1]} {b[2]} {b[3]} {b[4]} {b[5]} {b[6]}\n")
+        f.write(f"cfl {CFL}\niters {iters}\n")
+    out = os.path.join(cache, f"{workload}_ref.bin")
+    try:
+        r = subprocess.run([exe, case, su2, out, "solve"], capture_output=True, text=True, timeout=600)
+    except Exception as e:
+        return {"unavailable": str(e)[:200]}
+    import re
+    m = re.search(r"ref_driver: (\d+) iterations, ([0-9.eE+-]+) s wall, ([0-9.eE+-]+) cell-updates/s", r.stdout)
+    if r.returncode != 0 or not m:
+        return {"unavailable": (r.stderr or r.stdout)[-200:]}
+    return {"value": float(m.group(3)), "unit": "cell-updates/s", "iterations": int(m.group(1)),
+            "loop_seconds": float(m.group(2)),
+            "what": "the reference's PhysicsEuler loop from its own sources (built by oracle/Makefile.ref), "
+                    "same mesh and case, same GPU"}
 
 
 def main():
