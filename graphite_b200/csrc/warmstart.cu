@@ -40,7 +40,7 @@ namespace gb {
 namespace {
 
 constexpr int kTile = 128;                 // samples per tile = TMEM lanes
-constexpr int kThreads = 128;
+constexpr int kThreads = 256;              // two warps per TMEM lane quarter
 constexpr int kFeatures = 8;
 constexpr int kOutputs = 5;
 constexpr int kIn = 16;                    // padded input width (K of layer 1)
@@ -210,12 +210,16 @@ __device__ __forceinline__ void gemm(uint32_t d, uint32_t a, int a_cols, bool a_
     }
 }
 
-// Shared state of one CTA of the MLP kernels.
+// Shared state of one CTA of the MLP kernels.  Thread t works on row (sample
+// or hidden unit) `row` = its TMEM lane: warp w reads lane quarter w % 4;
+// the two warps of a quarter split the 128 columns of an epilogue (`half`).
 struct Cta {
     uint8_t* sm;              // generic pointer to the dynamic shared memory
     uint32_t sa;              // its shared address
     uint32_t tm;              // TMEM base
     uint32_t lane;            // this warp's TMEM lane offset (bits 16..)
+    int row;                  // TMEM lane = tile row of this thread
+    int half;                 // 0: columns 0..63 (and the per-row work), 1: columns 64..127
     uint64_t* bar;
     uint32_t phase;
 };
@@ -242,9 +246,9 @@ __device__ __forceinline__ bool stage(Cta& c, Issue issue) {
 
 // S (128 fp32 columns of this thread's row) -> silu -> bf16 row of buf
 __device__ __forceinline__ void epi_silu(const Cta& c, uint32_t s_col, uint8_t* buf) {
-    const int r = threadIdx.x;
+    const int r = c.row;
 #pragma unroll 1
-    for (int q = 0; q < 4; ++q) {
+    for (int q = 2 * c.half; q < 2 * c.half + 2; ++q) {
         float z[32];
         umma::ld32(c.tm + c.lane + s_col + 32u * q, z);
 #pragma unroll
@@ -256,9 +260,9 @@ __device__ __forceinline__ void epi_silu(const Cta& c, uint32_t s_col, uint8_t* 
 
 // dZ = dA * silu'(Z) with dA in S1, Z in S2 -> bf16 row of buf
 __device__ __forceinline__ void epi_dsilu(const Cta& c, uint8_t* buf) {
-    const int r = threadIdx.x;
+    const int r = c.row;
 #pragma unroll 1
-    for (int q = 0; q < 4; ++q) {
+    for (int q = 2 * c.half; q < 2 * c.half + 2; ++q) {
         float da[32], z[32];
         umma::ld32x2(c.tm + c.lane + kTmS1 + 32u * q, c.tm + c.lane + kTmS2 + 32u * q, da, z);
 #pragma unroll
@@ -272,8 +276,8 @@ __device__ __forceinline__ void epi_dsilu(const Cta& c, uint8_t* buf) {
 }
 
 // sample of this thread in tile `tile`: features f[8], targets tg[5]; false = padding row
-__device__ __forceinline__ bool load_sample(const Samples& s, int64_t tile, int field_fixed, float* f, float* tg) {
-    const int r = threadIdx.x;
+__device__ __forceinline__ bool load_sample(const Samples& s, int64_t tile, int field_fixed, int r, float* f,
+                                            float* tg) {
     if (s.x) {
         const int64_t i = tile * kTile + r;
         if (i >= s.n) return false;
@@ -305,13 +309,13 @@ __device__ __forceinline__ bool load_sample(const Samples& s, int64_t tile, int 
     return true;
 }
 
-__device__ __forceinline__ void put_x(uint8_t* sm, bool valid, const float* f) {
+__device__ __forceinline__ void put_x(uint8_t* sm, int r, bool valid, const float* f) {
     float v[8];
 #pragma unroll
     for (int k = 0; k < 8; ++k) v[k] = valid ? f[k] : 0.0f;
-    put8(sm + kSmX, kIn, threadIdx.x, 0, v);
+    put8(sm + kSmX, kIn, r, 0, v);
     const float zero[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-    put8(sm + kSmX, kIn, threadIdx.x, 1, zero);
+    put8(sm + kSmX, kIn, r, 1, zero);
 }
 
 __device__ __forceinline__ void cta_setup(Cta& c, uint8_t* sm, const uint4* img, uint64_t* bar, uint32_t* slot) {
@@ -326,7 +330,9 @@ __device__ __forceinline__ void cta_setup(Cta& c, uint8_t* sm, const uint4* img,
     __syncthreads();
     umma::fence_after_sync();
     c.tm = *slot;
-    c.lane = (uint32_t)((threadIdx.x >> 5) * 32) << 16;
+    c.lane = (uint32_t)(((threadIdx.x >> 5) & 3) * 32) << 16;
+    c.row = (int)(((threadIdx.x >> 5) & 3) * 32 + (threadIdx.x & 31));
+    c.half = (int)(threadIdx.x >> 7);
 }
 
 __device__ __forceinline__ void cta_teardown(Cta& c, TrainCtl* ctl, bool ok, int where) {
@@ -366,7 +372,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp_train(const TrainArgs a) {
     __shared__ uint32_t slot;
     Cta c;
     cta_setup(c, sm, a.img, &bar, &slot);
-    const int r = threadIdx.x;
+    const int r = c.row;
+    const bool rowwork = c.half == 0;   // the per-row work (sample, loss, thin layers) is done by half 0
     const uint32_t X = c.sa + kSmX, A1 = c.sa + kSmA1, A2 = c.sa + kSmA2, A3 = c.sa + kSmA3, DY = c.sa + kSmDY;
     const uint32_t W1 = c.sa + kImgW1, W2 = c.sa + kImgW2, W3 = c.sa + kImgW3, W4 = c.sa + kImgW4;
     const uint32_t S1 = c.tm + kTmS1, S2 = c.tm + kTmS2, DW2 = c.tm + kTmDW2, DW3 = c.tm + kTmDW3;
@@ -386,12 +393,15 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp_train(const TrainArgs a) {
             tile = permute_index(slot_id % a.s.n_tiles, a.s.n_tiles, a.seed ^ (0x9E3779B97F4A7C15ull * (epoch + 1)));
         }
         float f[8], tg[5] = {0, 0, 0, 0, 0};
-        const bool valid = load_sample(a.s, tile, -1, f, tg);
-        put_x(c.sm, valid, f);
+        bool valid = false;
+        if (rowwork) {
+            valid = load_sample(a.s, tile, -1, r, f, tg);
+            put_x(c.sm, r, valid, f);
+        }
         where = 1;
         if (!(ok = forward(c))) break;
         // loss gradient: dY = dy_scale * (y - t) on valid rows
-        {
+        if (rowwork) {
             float y[16];
             umma::ld16(S2 + c.lane, y);
             float dy[16];
@@ -411,7 +421,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp_train(const TrainArgs a) {
         where = 2;
         // dW4^T (this tile) = A3^T dY -> S2
         if (!(ok = stage(c, [&] { gemm(S2, A3, kHid, true, DY, kOutPad, true, 128, kOutPad, kTile, false); }))) break;
-        {
+        if (rowwork) {
             float v[16];
             umma::ld16(S2 + c.lane, v);
 #pragma unroll
@@ -447,7 +457,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp_train(const TrainArgs a) {
         where = 6;
         // dW1 (this tile) = dZ1^T X -> S1
         if (!(ok = stage(c, [&] { gemm(S1, A1, kHid, true, X, kIn, true, 128, kIn, kTile, false); }))) break;
-        {
+        if (rowwork) {
             float v[16];
             umma::ld16(S1 + c.lane, v);
 #pragma unroll
@@ -456,31 +466,32 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp_train(const TrainArgs a) {
     }
     if (ok) {
         float* P = a.partials + (size_t)blockIdx.x * kParams;
+        // half 0 drains dW2, half 1 dW3 (row r = output unit)
+        const uint32_t DW = rowwork ? DW2 : DW3;
+        float* Pw = P + (rowwork ? kOffW2 : kOffW3) + r * kHid;
 #pragma unroll 1
         for (int q = 0; q < 4; ++q) {
-            float v2[32], v3[32];
+            float v2[32];
             if (first) {
 #pragma unroll
-                for (int k = 0; k < 32; ++k) v2[k] = v3[k] = 0.0f;
+                for (int k = 0; k < 32; ++k) v2[k] = 0.0f;
             } else {
-                umma::ld32x2(DW2 + c.lane + 32u * q, DW3 + c.lane + 32u * q, v2, v3);
+                umma::ld32(DW + c.lane + 32u * q, v2);
             }
-            float4* p2 = reinterpret_cast<float4*>(P + kOffW2 + r * kHid + 32 * q);
-            float4* p3 = reinterpret_cast<float4*>(P + kOffW3 + r * kHid + 32 * q);
+            float4* p2 = reinterpret_cast<float4*>(Pw + 32 * q);
 #pragma unroll
-            for (int k = 0; k < 8; ++k) {
-                p2[k] = make_float4(v2[4 * k], v2[4 * k + 1], v2[4 * k + 2], v2[4 * k + 3]);
-                p3[k] = make_float4(v3[4 * k], v3[4 * k + 1], v3[4 * k + 2], v3[4 * k + 3]);
-            }
+            for (int k = 0; k < 8; ++k) p2[k] = make_float4(v2[4 * k], v2[4 * k + 1], v2[4 * k + 2], v2[4 * k + 3]);
         }
+        if (rowwork) {
 #pragma unroll
-        for (int k = 0; k < 16; ++k) {
-            P[kOffW1 + r * kIn + k] = acc1[k];
-            P[kOffW4 + k * kHid + r] = acc4[k];
+            for (int k = 0; k < 16; ++k) {
+                P[kOffW1 + r * kIn + k] = acc1[k];
+                P[kOffW4 + k * kHid + r] = acc4[k];
+            }
         }
         // loss partial (fixed order)
         __shared__ double red[kThreads];
-        red[r] = loss;
+        red[threadIdx.x] = loss;
         __syncthreads();
         if (r == 0) {
             double s = 0.0;
@@ -550,13 +561,17 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp_forward(const ForwardArgs a
     bool ok = true;
     for (int64_t tile = blockIdx.x; tile < n_tiles && ok; tile += gridDim.x) {
         float f[8], tg[5];
-        const bool valid = load_sample(a.s, tile, 0, f, tg);
-        put_x(c.sm, valid, f);
+        bool valid = false;
+        if (c.half == 0) {
+            valid = load_sample(a.s, tile, 0, c.row, f, tg);
+            put_x(c.sm, c.row, valid, f);
+        }
         if (!(ok = forward(c))) break;
+        if (c.half != 0) continue;
         float y[16];
         umma::ld16(c.tm + kTmS2 + c.lane, y);
         if (!valid) continue;
-        const int64_t i = tile * kTile + threadIdx.x;
+        const int64_t i = tile * kTile + c.row;
         if (a.y) {
 #pragma unroll
             for (int k = 0; k < kOutputs; ++k) a.y[i * kOutputs + k] = y[k];
