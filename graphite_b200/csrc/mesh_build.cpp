@@ -2,6 +2,7 @@
 // reference's cell/face/ghost topology, the .fvm file format, and the device
 // numbering (reverse Cuthill-McKee).
 #include <algorithm>
+#include <thread>
 #include <cerrno>
 #include <cstdio>
 #include <cstdlib>
@@ -212,10 +213,71 @@ struct FaceRec {
     uint32_t lf;
 };
 
+// Runs fn(lo, hi) over [0, n) split into contiguous ranges, one per host
+// thread (at most 32).
+template <typename Fn>
+void parallel_ranges(int64_t n, Fn fn) {
+    const unsigned hw = std::thread::hardware_concurrency();
+    const int64_t parts = std::max<int64_t>(1, std::min<int64_t>({(int64_t)(hw ? hw : 1), 32, n / 65536}));
+    if (parts == 1) {
+        fn((int64_t)0, n);
+        return;
+    }
+    std::vector<std::thread> th;
+    for (int64_t p = 0; p < parts; ++p) th.emplace_back(fn, n * p / parts, n * (p + 1) / parts);
+    for (auto& t : th) t.join();
+}
+
+inline bool rec_less(const FaceRec& x, const FaceRec& y) {
+    if (x.k0 != y.k0) return x.k0 < y.k0;
+    if (x.k1 != y.k1) return x.k1 < y.k1;
+    if (x.cell != y.cell) return x.cell < y.cell;   // records in (element, local face) order
+    return x.lf < y.lf;
+}
+
+// Sorts the records on the host's hardware threads: chunks sorted in
+// parallel, then merged pairwise, in parallel, log2(chunks) rounds.  The
+// order is total (no two records are equal), so the result is the same as a
+// serial sort's.
+void parallel_sort(std::vector<FaceRec>& v) {
+    const size_t n = v.size();
+    unsigned hw = std::thread::hardware_concurrency();
+    size_t chunks = 1;
+    while (chunks * 2 <= std::min<size_t>(hw ? hw : 1, 32) && n / (chunks * 2) >= 65536) chunks *= 2;
+    if (chunks == 1) {
+        std::sort(v.begin(), v.end(), rec_less);
+        return;
+    }
+    std::vector<size_t> cut(chunks + 1);
+    for (size_t c = 0; c <= chunks; ++c) cut[c] = n * c / chunks;
+    {
+        std::vector<std::thread> th;
+        for (size_t c = 0; c < chunks; ++c)
+            th.emplace_back([&, c] { std::sort(v.begin() + cut[c], v.begin() + cut[c + 1], rec_less); });
+        for (auto& t : th) t.join();
+    }
+    for (size_t w = 1; w < chunks; w *= 2) {
+        std::vector<std::thread> th;
+        for (size_t c = 0; c + w < chunks; c += 2 * w) {
+            const size_t lo = cut[c], mid = cut[c + w], hi = cut[std::min(c + 2 * w, chunks)];
+            th.emplace_back([&, lo, mid, hi] {
+                std::inplace_merge(v.begin() + lo, v.begin() + mid, v.begin() + hi, rec_less);
+            });
+        }
+        for (auto& t : th) t.join();
+    }
+}
+
 inline void make_key(const uint32_t* nodes, int n, uint64_t& k0, uint64_t& k1) {
     uint32_t s[4] = {0xffffffffu, 0xffffffffu, 0xffffffffu, 0xffffffffu};
     for (int i = 0; i < n; ++i) s[i] = nodes[i];
-    std::sort(s, s + n);
+    // 4-input sorting network; a triangle's padding (all ones) stays last
+    auto cx = [&](int a, int b) {
+        const uint32_t lo = std::min(s[a], s[b]), hi = std::max(s[a], s[b]);
+        s[a] = lo;
+        s[b] = hi;
+    };
+    cx(0, 1); cx(2, 3); cx(0, 2); cx(1, 3); cx(1, 2);
     k0 = ((uint64_t)s[0] << 32) | s[1];
     k1 = ((uint64_t)s[2] << 32) | s[3];
 }
@@ -223,7 +285,7 @@ inline void make_key(const uint32_t* nodes, int n, uint64_t& k0, uint64_t& k1) {
 }  // namespace
 
 // Conversion semantics of cuMeshFromSu2 (src/meshio.cu:713-764, 978-1136),
-// done by sorting face keys instead of a serial hash map.
+// done by a parallel sort of the face keys instead of a serial hash map.
 bool build_topology(const ElementSet& es, Topology& t) {
     const int64_t N = (int64_t)es.kinds.size();
     const int64_t G = (int64_t)es.bkinds.size();
@@ -236,28 +298,23 @@ bool build_topology(const ElementSet& es, Topology& t) {
     std::vector<int64_t> rec_off(N + 1, 0);
     for (int64_t e = 0; e < N; ++e) rec_off[e + 1] = rec_off[e] + local_faces(es.kinds[e])->n;
     const int64_t S = rec_off[N];
-    std::vector<FaceRec> rec(S);
-    for (int64_t e = 0; e < N; ++e) {
-        const LocalFaces* lf = local_faces(es.kinds[e]);
-        const uint32_t* en = es.enodes.data() + es.eoff[e];
-        for (int f = 0; f < lf->n; ++f) {
-            uint32_t fnodes[4];
-            for (int j = 0; j < lf->size[f]; ++j) fnodes[j] = en[lf->node[f][j]];
-            FaceRec& r = rec[rec_off[e] + f];
-            make_key(fnodes, lf->size[f], r.k0, r.k1);
-            r.cell = (uint32_t)e;
-            r.lf = (uint32_t)f;
+    std::vector<FaceRec> srt(S);
+    parallel_ranges(N, [&](int64_t e0, int64_t e1) {
+        for (int64_t e = e0; e < e1; ++e) {
+            const LocalFaces* lf = local_faces(es.kinds[e]);
+            const uint32_t* en = es.enodes.data() + es.eoff[e];
+            for (int f = 0; f < lf->n; ++f) {
+                uint32_t fnodes[4];
+                for (int j = 0; j < lf->size[f]; ++j) fnodes[j] = en[lf->node[f][j]];
+                FaceRec& r = srt[rec_off[e] + f];
+                make_key(fnodes, lf->size[f], r.k0, r.k1);
+                r.cell = (uint32_t)e;
+                r.lf = (uint32_t)f;
+            }
         }
-    }
-    std::vector<uint32_t> order(S);
-    std::iota(order.begin(), order.end(), 0u);
-    std::sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) {
-        const FaceRec& x = rec[a];
-        const FaceRec& y = rec[b];
-        if (x.k0 != y.k0) return x.k0 < y.k0;
-        if (x.k1 != y.k1) return x.k1 < y.k1;
-        return a < b;   // records are in (element, local face) order
     });
+    parallel_sort(srt);
+    auto rec_index = [&](const FaceRec& r) { return (uint32_t)(rec_off[r.cell] + r.lf); };
     // groups of equal keys
     std::vector<uint32_t> group_of(S);
     std::vector<uint64_t> gk0, gk1;
@@ -265,11 +322,12 @@ bool build_topology(const ElementSet& es, Topology& t) {
     std::vector<uint32_t> g_cells;      // 2 per group
     std::vector<uint8_t> g_count;
     for (int64_t i = 0; i < S; ++i) {
-        const FaceRec& r = rec[order[i]];
+        const FaceRec& r = srt[i];
+        const uint32_t ri = rec_index(r);
         if (i == 0 || r.k0 != gk0.back() || r.k1 != gk1.back()) {
             gk0.push_back(r.k0);
             gk1.push_back(r.k1);
-            g_first.push_back(order[i]);
+            g_first.push_back(ri);
             g_cells.push_back(r.cell);
             g_cells.push_back(0xffffffffu);
             g_count.push_back(1);
@@ -283,8 +341,9 @@ bool build_topology(const ElementSet& es, Topology& t) {
             g_cells[2 * g + 1] = r.cell;
             g_count[g] = 2;
         }
-        group_of[order[i]] = (uint32_t)(gk0.size() - 1);
+        group_of[ri] = (uint32_t)(gk0.size() - 1);
     }
+    std::vector<FaceRec>().swap(srt);
     const int64_t F = (int64_t)gk0.size();
     t.F = F;
     // ghosts: one per boundary face, ids N + (running index), by region
@@ -318,43 +377,76 @@ bool build_topology(const ElementSet& es, Topology& t) {
             return false;
         }
     }
-    // face ids in order of first appearance; node order of the creator
+    // face ids in order of first appearance; node order of the creator.
+    // Pass 1 counts each element range's creating faces and their nodes, a
+    // prefix sum gives each range its first face id and node offset, pass 2
+    // writes them.
+    const unsigned hw = std::thread::hardware_concurrency();
+    const int64_t parts = std::max<int64_t>(1, std::min<int64_t>({(int64_t)(hw ? hw : 1), 32, N / 65536}));
+    std::vector<int64_t> p_faces(parts + 1, 0), p_nodes(parts + 1, 0);
+    auto creates = [&](int64_t e, int f) {
+        const uint32_t ri = (uint32_t)(rec_off[e] + f);
+        return g_first[group_of[ri]] == ri;
+    };
+    auto over_parts = [&](auto fn) {
+        std::vector<std::thread> th;
+        for (int64_t p = 0; p < parts; ++p) th.emplace_back(fn, p, N * p / parts, N * (p + 1) / parts);
+        for (auto& x : th) x.join();
+    };
+    over_parts([&](int64_t p, int64_t e0, int64_t e1) {
+        int64_t nf = 0, nn = 0;
+        for (int64_t e = e0; e < e1; ++e) {
+            const LocalFaces* lf = local_faces(es.kinds[e]);
+            for (int f = 0; f < lf->n; ++f)
+                if (creates(e, f)) { ++nf; nn += lf->size[f]; }
+        }
+        p_faces[p + 1] = nf;
+        p_nodes[p + 1] = nn;
+    });
+    for (int64_t p = 0; p < parts; ++p) {
+        p_faces[p + 1] += p_faces[p];
+        p_nodes[p + 1] += p_nodes[p];
+    }
+    if (p_faces[parts] != F) {
+        set_error("internal error: face count mismatch in the topology builder");
+        return false;
+    }
     std::vector<uint32_t> fid(F, 0xffffffffu);
-    uint32_t next = 0;
-    t.fns.assign(1, 0);
-    t.fns.reserve(F + 1);
-    t.fn.reserve(S * 3);
-    for (int64_t e = 0; e < N; ++e) {
-        const LocalFaces* lf = local_faces(es.kinds[e]);
-        const uint32_t* en = es.enodes.data() + es.eoff[e];
-        for (int f = 0; f < lf->n; ++f) {
-            const uint32_t ri = (uint32_t)(rec_off[e] + f);
-            const uint32_t g = group_of[ri];
-            if (g_first[g] != ri) continue;
-            fid[g] = next++;
-            for (int j = 0; j < lf->size[f]; ++j) t.fn.push_back(en[lf->node[f][j]]);
-            t.fns.push_back((uint32_t)t.fn.size());
+    t.fns.assign(F + 1, 0);
+    t.fn.assign(p_nodes[parts], 0);
+    over_parts([&](int64_t p, int64_t e0, int64_t e1) {
+        int64_t next = p_faces[p], pos = p_nodes[p];
+        for (int64_t e = e0; e < e1; ++e) {
+            const LocalFaces* lf = local_faces(es.kinds[e]);
+            const uint32_t* en = es.enodes.data() + es.eoff[e];
+            for (int f = 0; f < lf->n; ++f) {
+                if (!creates(e, f)) continue;
+                fid[group_of[rec_off[e] + f]] = (uint32_t)next;
+                for (int j = 0; j < lf->size[f]; ++j) t.fn[pos++] = en[lf->node[f][j]];
+                t.fns[++next] = (uint32_t)pos;
+            }
         }
-    }
+    });
     // CSR, element-local face order (src/meshio.cu:1044-1136)
-    t.cfs.assign(1, 0);
-    t.cfs.reserve(N + G + 1);
-    t.cf.reserve(S + G);
-    t.cc.reserve(S + G);
-    for (int64_t e = 0; e < N; ++e) {
-        for (int64_t r = rec_off[e]; r < rec_off[e + 1]; ++r) {
-            const uint32_t g = group_of[r];
-            t.cf.push_back(fid[g]);
-            const uint32_t a = g_cells[2 * g], b = g_cells[2 * g + 1];
-            t.cc.push_back(a == (uint32_t)e ? b : a);
+    t.cfs.assign(N + G + 1, 0);
+    t.cf.assign(S + G, 0);
+    t.cc.assign(S + G, 0);
+    parallel_ranges(N, [&](int64_t e0, int64_t e1) {
+        for (int64_t e = e0; e < e1; ++e) {
+            for (int64_t r = rec_off[e]; r < rec_off[e + 1]; ++r) {
+                const uint32_t g = group_of[r];
+                t.cf[r] = fid[g];
+                const uint32_t a = g_cells[2 * g], b = g_cells[2 * g + 1];
+                t.cc[r] = a == (uint32_t)e ? b : a;
+            }
+            t.cfs[e + 1] = (uint32_t)rec_off[e + 1];
         }
-        t.cfs.push_back((uint32_t)t.cf.size());
-    }
+    });
     for (int64_t b = 0; b < G; ++b) {
         const uint32_t g = bgroup[b];
-        t.cf.push_back(fid[g]);
-        t.cc.push_back(g_cells[2 * g]);
-        t.cfs.push_back((uint32_t)t.cf.size());
+        t.cf[S + b] = fid[g];
+        t.cc[S + b] = g_cells[2 * g];
+        t.cfs[N + b + 1] = (uint32_t)(S + b + 1);
     }
     t.ghost_ids.resize(G);
     for (int64_t b = 0; b < G; ++b) t.ghost_ids[b] = (uint32_t)(N + b);

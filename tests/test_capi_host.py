@@ -53,6 +53,29 @@ def test_converter_matches_reference_converter(name, su2_paths, workdir):
     assert rr == mr
 
 
+def test_parallel_converter_matches_oracle_topology(workdir):
+    """At 216k elements the converter builds the face records, sorts them and
+    numbers the faces on several host threads; its file equals the oracle's
+    serial topology (both number faces in first-appearance order) exactly."""
+    from graphite_b200 import meshgen
+    from oracle import OracleMesh
+    mesh = meshgen.channel_bump(nx=60, ny=30, nz=20, cells="tet")
+    su2, out = str(workdir / "par.su2"), str(workdir / "par.fvm")
+    mesh.write_su2(su2)
+    assert capi.load().cuMeshFromSu2(su2.encode(), out.encode()) == 0, capi.last_error()
+    nodes, faces, cells, regions = read_fvm(out)
+    om = OracleMesh(mesh, metric_bits=64)
+    assert (len(cells), len(faces)) == (om.N + om.G, om.F)
+    fs, fn = om.get("face_nodes_starts"), om.get("face_nodes")
+    assert np.array_equal(np.cumsum([0] + [len(f) for f in faces]), fs)
+    assert np.array_equal(np.concatenate([np.array(f) for f in faces]), fn)
+    cs = om.get("cell_faces_starts")
+    assert np.array_equal(np.cumsum([0] + [len(c[0]) for c in cells]), cs)
+    assert np.array_equal(np.concatenate([np.array(c[0]) for c in cells]), om.get("cell_faces"))
+    assert np.array_equal(np.concatenate([np.array(c[1]) for c in cells]), om.get("cell_connects"))
+    assert [r[0] for r in regions] == list(mesh.markers)
+
+
 def _write(path, text):
     with open(path, "w") as f:
         f.write(text)
