@@ -62,12 +62,16 @@ struct BcDev {
     float p, t;
 };
 
-// Two register budgets for the batched gradient / flux kernels (resident
-// 256-thread blocks per SM): variant 0 keeps every value in registers,
-// variant 1 trades a few spills for one more resident block.  The autotuner
-// picks one.
+// Three forms of the batched gradient / flux kernels: variant 0 and 1 are
+// two register budgets (resident 256-thread blocks per SM; 1 trades a few
+// spills for one more resident block), variant 2 runs the gradient pass in
+// 64-thread blocks that stage each cell's per-face entries in shared memory
+// with cp.async (flux as in variant 1).  The autotuner picks one.
 constexpr int kBatchGradBlocks[2] = {4, 5};
 constexpr int kBatchFluxBlocks[2] = {4, 5};
+constexpr int kBatchVariants = 3;
+constexpr int kStagedThreads = 64;
+constexpr int kStagedBlocks = 14;
 
 __global__ void k_batch_bc(const int2* __restrict__ items, int n_items, InstDev* insts,
                            const MeshTab* __restrict__ meshes, const BcDev* __restrict__ bcs) {
@@ -111,6 +115,39 @@ __global__ void __launch_bounds__(kBlock, BLOCKS)
     const uint32_t c0 = (uint32_t)w.y * tile;
     const uint32_t c1 = min(m.N, c0 + (uint32_t)tile);
     for (uint32_t i = c0 + threadIdx.x; i < c1; i += blockDim.x) grad_lim_cell<TRANSPOSED>(m, q, g, i);
+}
+
+template <bool TRANSPOSED>
+__global__ void __launch_bounds__(kStagedThreads, kStagedBlocks)
+    k_batch_grad_staged(const int2* __restrict__ items, const InstDev* insts, const MeshTab* __restrict__ meshes,
+                        int tile) {
+    constexpr int B = kStagedThreads;
+    __shared__ float4 s_dn[kSlots * B], s_df[kSlots * B];
+    __shared__ uint32_t s_nbc[kSlots * B], s_twin[kSlots * B];
+    const int2 w = items[blockIdx.x];
+    const InstDev& I = insts[w.x];
+    if (I.status) return;
+    const MeshDev m = meshes[I.mesh].m;
+    const int cur = I.cur;
+    const EulerState q{I.rho[cur], I.rhou[cur], I.rhoe[cur]};
+    const EulerGrad g{nullptr, nullptr, nullptr, I.rec_rho, I.rec_rhou};
+    const uint32_t c0 = (uint32_t)w.y * tile;
+    const uint32_t c1 = min(m.N, c0 + (uint32_t)tile);
+    const uint32_t tid = threadIdx.x;
+    // the slots are this thread's own; the previous cell's reads of them have
+    // completed before its results were stored
+    for (uint32_t i = c0 + tid; i < c1; i += B) {
+        const uint32_t nf = __ldg(&m.nfc[i]);
+        for (uint32_t t = 0; t < nf; ++t) {
+            const uint32_t k = i + t * m.N;
+            cp_async4(&s_nbc[t * B + tid], &m.nbc[k]);
+            cp_async16(&s_dn[t * B + tid], &m.dn[k]);
+            cp_async16(&s_df[t * B + tid], &m.df[k]);
+            cp_async4(&s_twin[t * B + tid], &m.twin[k]);
+        }
+        asm volatile("cp.async.commit_group;\n" ::: "memory");
+        grad_lim_cell<TRANSPOSED>(m, q, g, i, nf, EntriesStaged<B>{s_nbc + tid, s_dn + tid, s_df + tid, s_twin + tid});
+    }
 }
 
 template <int BLOCKS>
@@ -297,9 +334,13 @@ void enqueue_iteration(Batch* b, float cfl, double tol, cudaStream_t s) {
             if (tr) k_batch_grad<true, kBatchGradBlocks[0]><<<n, kBlock, 0, s>>>(b->d_cell_items, b->d_inst, b->d_mesh, b->tile);
             else k_batch_grad<false, kBatchGradBlocks[0]><<<n, kBlock, 0, s>>>(b->d_cell_items, b->d_inst, b->d_mesh, b->tile);
             k_batch_flux<kBatchFluxBlocks[0]><<<n, kBlock, 0, s>>>(b->d_cell_items, b->d_inst, b->d_mesh, b->tile, cfl);
-        } else {
+        } else if (b->variant == 1) {
             if (tr) k_batch_grad<true, kBatchGradBlocks[1]><<<n, kBlock, 0, s>>>(b->d_cell_items, b->d_inst, b->d_mesh, b->tile);
             else k_batch_grad<false, kBatchGradBlocks[1]><<<n, kBlock, 0, s>>>(b->d_cell_items, b->d_inst, b->d_mesh, b->tile);
+            k_batch_flux<kBatchFluxBlocks[1]><<<n, kBlock, 0, s>>>(b->d_cell_items, b->d_inst, b->d_mesh, b->tile, cfl);
+        } else {
+            if (tr) k_batch_grad_staged<true><<<n, kStagedThreads, 0, s>>>(b->d_cell_items, b->d_inst, b->d_mesh, b->tile);
+            else k_batch_grad_staged<false><<<n, kStagedThreads, 0, s>>>(b->d_cell_items, b->d_inst, b->d_mesh, b->tile);
             k_batch_flux<kBatchFluxBlocks[1]><<<n, kBlock, 0, s>>>(b->d_cell_items, b->d_inst, b->d_mesh, b->tile, cfl);
         }
     }
@@ -516,8 +557,8 @@ int gbBatchGetState(gbBatch* b, int inst, float* rho, float* rhou, float* rhoe) 
 
 int gbBatchSetTuning(gbBatch* b, int tile_cells, int schedule) {
     clear_error();
-    if (!b || tile_cells < kBlock || tile_cells % kBlock || schedule < 0 || schedule > 3) {
-        set_error("gbBatchSetTuning: tile must be a positive multiple of 256, schedule 0..3");
+    if (!b || tile_cells < kBlock || tile_cells % kBlock || schedule < 0 || schedule >= 2 * kBatchVariants) {
+        set_error("gbBatchSetTuning: tile must be a positive multiple of 256, schedule 0..5");
         return 1;
     }
     b->tile = tile_cells;
@@ -562,7 +603,7 @@ int gbBatchAutotune(gbBatch* b, gb_scalar cfl, int trial_iters, int* tile_out, i
         float best = 1e30f;
         Tuning best_t{b->tile, b->schedule, b->variant};
         const int tiles[] = {256, 512, 1024, 2048};
-        for (int var = 0; var < 2 && ok; ++var)
+        for (int var = 0; var < kBatchVariants && ok; ++var)
         for (int sched = 0; sched < 2 && ok; ++sched) {
             for (int tile : tiles) {
                 if (!ok) break;

@@ -25,6 +25,9 @@ namespace {
 #ifndef GB_FLUX_BLOCKS
 #define GB_FLUX_BLOCKS 6
 #endif
+#ifndef GB_GRAD_STAGED
+#define GB_GRAD_STAGED 1
+#endif
 #ifndef GB_GRAD_BLOCKS
 #define GB_GRAD_BLOCKS 5
 #endif
@@ -84,6 +87,39 @@ template <bool TRANSPOSED>
 __global__ void __launch_bounds__(kBlock, kGradBlocksPerSM) k_grad_lim(MeshDev m, EulerState q, EulerGrad g) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < m.N) grad_lim_cell<TRANSPOSED>(m, q, g, i);
+}
+
+// k_grad_lim with each cell's per-face entries (neighbour, LSQ offset, face
+// offset, twin) staged in shared memory by cp.async as the first thing the
+// thread does: all of a cell's entry streams are in flight together while the
+// cell's own state loads, instead of one face per memory round trip.
+#ifndef GB_GRAD_STAGE_THREADS
+#define GB_GRAD_STAGE_THREADS 64
+#endif
+#ifndef GB_GRAD_STAGE_BLOCKS
+#define GB_GRAD_STAGE_BLOCKS 14
+#endif
+constexpr int kStageThreads = GB_GRAD_STAGE_THREADS;
+
+template <bool TRANSPOSED>
+__global__ void __launch_bounds__(kStageThreads, GB_GRAD_STAGE_BLOCKS)
+    k_grad_lim_staged(MeshDev m, EulerState q, EulerGrad g) {
+    constexpr int B = kStageThreads;
+    __shared__ float4 s_dn[kSlots * B], s_df[kSlots * B];
+    __shared__ uint32_t s_nbc[kSlots * B], s_twin[kSlots * B];
+    const uint32_t tid = threadIdx.x;
+    const uint32_t i = blockIdx.x * B + tid;
+    if (i >= m.N) return;
+    const uint32_t nf = __ldg(&m.nfc[i]);
+    for (uint32_t t = 0; t < nf; ++t) {
+        const uint32_t k = i + t * m.N;
+        cp_async4(&s_nbc[t * B + tid], &m.nbc[k]);
+        cp_async16(&s_dn[t * B + tid], &m.dn[k]);
+        cp_async16(&s_df[t * B + tid], &m.df[k]);
+        cp_async4(&s_twin[t * B + tid], &m.twin[k]);
+    }
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+    grad_lim_cell<TRANSPOSED>(m, q, g, i, nf, EntriesStaged<B>{s_nbc + tid, s_dn + tid, s_df + tid, s_twin + tid});
 }
 
 // Fused flux / local-time-step update / squared residual over the interior
@@ -193,8 +229,14 @@ void launch_entry_geo(const DevMesh& m, cudaStream_t s) {
 
 void launch_grad_lim(const DevMesh& m, EulerState q, EulerGrad g, bool transposed, cudaStream_t s) {
     if (m.N == 0) return;
+#if GB_GRAD_STAGED
+    const unsigned gs = (unsigned)((m.N + kStageThreads - 1) / kStageThreads);
+    if (transposed) k_grad_lim_staged<true><<<gs, kStageThreads, 0, s>>>(mesh_dev(m), q, g);
+    else k_grad_lim_staged<false><<<gs, kStageThreads, 0, s>>>(mesh_dev(m), q, g);
+#else
     if (transposed) k_grad_lim<true><<<grid(m.N), kBlock, 0, s>>>(mesh_dev(m), q, g);
     else k_grad_lim<false><<<grid(m.N), kBlock, 0, s>>>(mesh_dev(m), q, g);
+#endif
     count_launch();
 }
 

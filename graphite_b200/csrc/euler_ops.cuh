@@ -167,31 +167,68 @@ __device__ __forceinline__ void farfield_ghost(const float4* __restrict__ cell_g
     ru4 = make_float4(ru.x, ru.y, ru.z, 0.f);
 }
 
+// Per-face entry data of cell i (slot t = 0..nf-1), read straight from the
+// slot-major arrays at entry i + t N.
+struct EntriesGlobal {
+    const MeshDev& m;
+    uint32_t i;
+    __device__ __forceinline__ uint32_t nbc(uint32_t t) const { return __ldg(&m.nbc[i + t * m.N]); }
+    __device__ __forceinline__ float4 dn(uint32_t t) const { return __ldg(&m.dn[i + t * m.N]); }
+    __device__ __forceinline__ float4 df(uint32_t t) const { return __ldg(&m.df[i + t * m.N]); }
+    __device__ __forceinline__ uint32_t twin(uint32_t t) const { return __ldg(&m.twin[i + t * m.N]); }
+    __device__ __forceinline__ void ready() const {}
+};
+
+// The same entries copied by this thread into its own shared-memory slots
+// (slot t at t * B past the thread's base) with cp.async: every face's
+// stream is in flight at once instead of one face at a time.
+template <int B>
+struct EntriesStaged {
+    const uint32_t* s_nbc;
+    const float4* s_dn;
+    const float4* s_df;
+    const uint32_t* s_twin;
+    __device__ __forceinline__ uint32_t nbc(uint32_t t) const { return s_nbc[t * B]; }
+    __device__ __forceinline__ float4 dn(uint32_t t) const { return s_dn[t * B]; }
+    __device__ __forceinline__ float4 df(uint32_t t) const { return s_df[t * B]; }
+    __device__ __forceinline__ uint32_t twin(uint32_t t) const { return s_twin[t * B]; }
+    __device__ __forceinline__ void ready() const { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+};
+
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+    const uint32_t a = (uint32_t)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(a), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
+    const uint32_t a = (uint32_t)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(a), "l"(gmem) : "memory");
+}
+
 // Fused FvmEulerStepPrepare for one interior cell i (src/models/euler.cu:597-647):
 // least-squares gradients (src/fvmops.cu:51-111) and limiters
 // (src/fvmops.cu:175-266) of rho, rhou (3 components) and rhoE, then the
 // limited reconstruction q + lim (grad q . d) of the cell at each of its faces
 // (the face states of fvmEulerSteadyOp, src/models/euler.cu:250-255) and of
 // each ghost neighbour, which carries this cell's gradient and limiter
-// (fvmScalGradLimBc / fvmVecGradLimBc, src/fvmops.cu:272-304).
-template <bool TRANSPOSED>
-__device__ __forceinline__ void grad_lim_cell(const MeshDev& m, EulerState q, EulerGrad g, uint32_t i) {
-    const float3 ci = f3(__ldg(&m.cell_geo[i]));
+// (fvmScalGradLimBc / fvmVecGradLimBc, src/fvmops.cu:272-304).  nf is the
+// cell's face count; e supplies its entries.
+template <bool TRANSPOSED, typename Entries>
+__device__ __forceinline__ void grad_lim_cell(const MeshDev& m, EulerState q, EulerGrad g, uint32_t i, uint32_t nf,
+                                              const Entries& e) {
     float v[5];
     float4 u0;
     {
         u0 = __ldg(&q.rhou[i]);
         v[0] = __ldg(&q.rho[i]); v[1] = u0.x; v[2] = u0.y; v[3] = u0.z; v[4] = __ldg(&q.rhoe[i]);
     }
+    e.ready();
     float3 gs[5];
     float vmin[5], vmax[5];
 #pragma unroll
     for (int c = 0; c < 5; ++c) { gs[c] = make_float3(0.f, 0.f, 0.f); vmin[c] = v[c]; vmax[c] = v[c]; }
-    const uint32_t nf = __ldg(&m.nfc[i]);
-    const uint32_t kend = i + nf * m.N;
-    for (uint32_t k = i; k < kend; k += m.N) {
-        const uint32_t j = __ldg(&m.nbc[k]);
-        const float4 dw = __ldg(&m.dn[k]);           // (c_j - c_i, 1 / |c_j - c_i|^2)
+    for (uint32_t t = 0; t < nf; ++t) {
+        const uint32_t j = e.nbc(t);
+        const float4 dw = e.dn(t);                   // (c_j - c_i, 1 / |c_j - c_i|^2)
         const float3 d = f3(dw);
         const float4 uj = __ldg(&q.rhou[j]);
         const float vj[5] = {__ldg(&q.rho[j]), uj.x, uj.y, uj.z, __ldg(&q.rhoe[j])};
@@ -206,8 +243,8 @@ __device__ __forceinline__ void grad_lim_cell(const MeshDev& m, EulerState q, Eu
 #pragma unroll
     for (int c = 0; c < 5; ++c) gs[c] = sym_mul(l0, l1, gs[c]);
     float lim[5] = {2.f, 2.f, 2.f, 2.f, 2.f};
-    for (uint32_t k = i; k < kend; k += m.N) {
-        const float4 dk = __ldg(&m.df[k]);           // (f_c - c_i, |f_c - c_i|^3)
+    for (uint32_t t = 0; t < nf; ++t) {
+        const float4 dk = e.df(t);                   // (f_c - c_i, |f_c - c_i|^3)
 #pragma unroll
         for (int c = 0; c < 5; ++c) lim[c] = fminf(lim[c], limiter(v[c], gs[c], vmin[c], vmax[c], f3(dk), dk.w));
     }
@@ -223,23 +260,29 @@ __device__ __forceinline__ void grad_lim_cell(const MeshDev& m, EulerState q, Eu
         g.rhou[3 * i + 2] = gu[2];
         g.rhoe[i] = ge;
     }
-    for (uint32_t k = i; k < kend; k += m.N) {
+    for (uint32_t t = 0; t < nf; ++t) {
+        const uint32_t k = i + t * m.N;
         float rr, re;
         float3 ru;
-        reconstruct<TRANSPOSED>(v[0], u0, v[4], gr, gu, ge, f3(__ldg(&m.df[k])), rr, ru, re);
+        reconstruct<TRANSPOSED>(v[0], u0, v[4], gr, gu, ge, f3(e.df(t)), rr, ru, re);
         g.rec_rho[k] = rr;
         g.rec_rhou[k] = make_float4(ru.x, ru.y, ru.z, re);
-        const uint32_t t = __ldg(&m.twin[k]);
-        if (t >= m.S) {
+        const uint32_t tw = e.twin(t);
+        if (tw >= m.S) {
             // ghost neighbour: its state with this cell's gradient and limiter
-            const uint32_t j = m.N + (t - m.S);
+            const uint32_t j = m.N + (tw - m.S);
             const float3 fc = f3(__ldg(&m.face_geo[2 * __ldg(&m.nb[k]).x + 1]));
             reconstruct<TRANSPOSED>(__ldg(&q.rho[j]), __ldg(&q.rhou[j]), __ldg(&q.rhoe[j]), gr, gu, ge,
                                     fc - f3(__ldg(&m.cell_geo[j])), rr, ru, re);
-            g.rec_rho[t] = rr;
-            g.rec_rhou[t] = make_float4(ru.x, ru.y, ru.z, re);
+            g.rec_rho[tw] = rr;
+            g.rec_rhou[tw] = make_float4(ru.x, ru.y, ru.z, re);
         }
     }
+}
+
+template <bool TRANSPOSED>
+__device__ __forceinline__ void grad_lim_cell(const MeshDev& m, EulerState q, EulerGrad g, uint32_t i) {
+    grad_lim_cell<TRANSPOSED>(m, q, g, i, __ldg(&m.nfc[i]), EntriesGlobal{m, i});
 }
 
 // Fused fvmEulerSteadyOp + euler_steady_step for one interior cell i

@@ -638,7 +638,7 @@ void number_cells(const Topology& t, bool rcm, Numbering& num) {
                 std::sort(nbrs.begin(), nbrs.end(), [&](uint32_t a, uint32_t b) {
                     return deg[a] != deg[b] ? deg[a] < deg[b] : a < b;
                 });
-                order.insert(order.end(), nbrs.begin(), nbrs.end());
+                for (uint32_t v : nbrs) order.push_back(v);
             }
         }
         std::reverse(order.begin(), order.end());

@@ -279,9 +279,11 @@ int gbBatchSetState(gbBatch* batch, int instance, const float* rho, const float*
 int gbBatchGetState(gbBatch* batch, int instance, float* rho, float* rhou, float* rhoe);
 
 /* Work decomposition: cells per work item (multiple of 256) and schedule =
- * order + 2 * register variant; order 0 runs instance by instance, 1 tile by
- * tile across the instances of a mesh; variant 0 / 1 compiles the gradient
- * and flux kernels for 3 / 4 and 2 / 3 resident blocks per SM. */
+ * order + 2 * kernel variant (schedule 0..5); order 0 runs instance by
+ * instance, 1 tile by tile across the instances of a mesh; variant 0 / 1
+ * compiles the gradient and flux kernels for 4 / 5 resident 256-thread blocks
+ * per SM, variant 2 runs the gradient pass in 64-thread blocks that stage
+ * each cell's face entries in shared memory (flux as variant 1). */
 int gbBatchSetTuning(gbBatch* batch, int tile_cells, int schedule);
 int gbBatchGetTuning(gbBatch* batch, int* tile_cells, int* schedule);
 

@@ -33,7 +33,7 @@ def _instances():
     return [(k % 2, float(rng.uniform(0.3, 0.8)), float(rng.uniform(-2, 6))) for k in range(5)]
 
 
-@pytest.mark.parametrize("tuning", [(256, 0), (512, 1), (1024, 3), (2048, 2)])
+@pytest.mark.parametrize("tuning", [(256, 0), (512, 1), (1024, 3), (2048, 2), (512, 4), (1024, 5)])
 def test_batch_equals_plain_solves(meshes, tuning):
     """Every instance of a batch follows, bit for bit, the iterates of a plain
     solve of it, whatever the tile size and schedule."""
@@ -69,7 +69,7 @@ def test_batch_instances_stop_at_their_own_tolerance(meshes):
     spec = [(k, airfoil_bcs(m, a)[1]) for k, m, a in inst]
     with EulerBatch(cs, spec) as b:
         tile, sched = b.autotune(0.8, trial_iters=3)
-        assert tile % 256 == 0 and sched in (0, 1, 2, 3)
+        assert tile % 256 == 0 and sched in range(6)
         for i, (k, m, a) in enumerate(inst):
             b.init_uniform(i, airfoil_bcs(m, a)[0], cases.P_INF, cases.T_INF)
         done, its, rat, st, hist = b.run(0.8, 3000, tolerance=1e-2, check_every=50, history=True)
