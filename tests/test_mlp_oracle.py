@@ -85,7 +85,10 @@ def test_adam_matches_torch():
         opt.zero_grad()
         wt.grad = torch.from_numpy(g.copy())
         opt.step()
-    np.testing.assert_allclose(ww[~pad], wt.detach().numpy()[~pad], rtol=1e-12, atol=1e-15)
+    # torch's CPU Adam may take a vectorised path (FMA contraction depends on
+    # the tensor's alignment): allow ulp-level differences over 5 steps; a
+    # formula difference shows at 1e-4 and above
+    np.testing.assert_allclose(ww[~pad], wt.detach().numpy()[~pad], rtol=1e-9, atol=1e-13)
 
 
 def test_point_triangle_distance_against_sampling():
