@@ -347,8 +347,27 @@ void enqueue_iteration(Batch* b, float cfl, double tol, cudaStream_t s) {
     k_batch_reduce<<<b->n_inst, kBlock, 0, s>>>(b->d_inst, tol);
 }
 
+// Cells per work item while only some instances are still iterating: the
+// tuned tile, halved (down to 256) until the active instances give at least
+// 4 items per SM, so that a last slow instance still spreads over the GPU.
+int active_tile(const Batch* b, int tuned) {
+    const int64_t target = 4 * (int64_t)sm_count();
+    int t = tuned;
+    for (;;) {
+        int64_t items = 0;
+        for (int i = 0; i < b->n_inst; ++i)
+            if (b->h_inst[i].status == 0) items += tiles_of(b, i, t);
+        const int half = (t / 2) / kBlock * kBlock;
+        if (items >= target || half < kBlock) return t;
+        t = half;
+    }
+}
+
 // Runs up to max_iter iterations (graph replay, status polled every
-// check_every); per-instance state lives in d_inst.
+// check_every); per-instance state lives in d_inst.  When instances stop,
+// their work leaves the item list and the tile shrinks (active_tile); the
+// tuned tile is restored on return.  The states do not depend on the tile;
+// the residual's float64 block sums are then taken over smaller blocks.
 int64_t run_loop(Batch* b, float cfl, int64_t max_iter, double tol, int check_every) {
     cudaStream_t s = (cudaStream_t)gbGetStream();
     cudaStream_t cap = nullptr;
@@ -368,6 +387,7 @@ int64_t run_loop(Batch* b, float cfl, int64_t max_iter, double tol, int check_ev
         return good;
     };
     ok = ok && build_items(b) && capture();
+    const int tuned = b->tile;
     int64_t done = 0;
     int active = b->n_inst;
     while (ok && done < max_iter) {
@@ -384,11 +404,20 @@ int64_t run_loop(Batch* b, float cfl, int64_t max_iter, double tol, int check_ev
         if (now == 0) break;
         if (now != active) {             // drop the frozen instances' work
             active = now;
-            ok = build_items(b) && ok_(cudaStreamSynchronize(s), "batch items") && capture();
+            const int t = active_tile(b, tuned);
+            if (t != b->tile) {
+                b->tile = t;
+                ok = size_partials(b) && upload_inst(b);
+            }
+            ok = ok && build_items(b) && ok_(cudaStreamSynchronize(s), "batch items") && capture();
         }
     }
     if (exec) cudaGraphExecDestroy(exec);
     if (cap) cudaStreamDestroy(cap);
+    if (ok && b->tile != tuned) {        // nothing is in flight: download_inst synchronised
+        b->tile = tuned;
+        ok = size_partials(b) && upload_inst(b) && ok_(cudaStreamSynchronize(s), "batch table");
+    }
     return ok ? done : -1;
 }
 

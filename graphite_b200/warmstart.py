@@ -137,7 +137,7 @@ class WarmStart:
 
 
 def solve_warm(batch, ws_per_instance: Sequence[Optional[WarmStart]], cases: Sequence[tuple], cfl: float,
-               max_iter: int, tolerance: float, check_every: int = 100):
+               max_iter: int, tolerance: float, check_every: int = 25):
     """Warm-started batched solve.
 
     cases[i] = (mach vector, pressure, temperature) of instance i;

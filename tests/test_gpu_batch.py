@@ -63,6 +63,36 @@ def test_batch_equals_plain_solves(meshes, tuning):
         c.close()
 
 
+def test_tile_shrinks_as_instances_stop_without_changing_states(meshes):
+    """Once instances stop, the run re-tiles the remaining work into smaller
+    items; every instance still ends bit for bit where a plain solve of its
+    own iteration count ends, and the tuned tile is back after the run."""
+    lib = capi.load()
+    lib.gbSetReferenceMomentumReconstruction(1)
+    cs = [EulerCase(p) for p in meshes]
+    inst = _instances()
+    spec = [(k, airfoil_bcs(m, a)[1]) for k, m, a in inst]
+    with EulerBatch(cs, spec) as b:
+        b.set_tuning(2048, 5)
+        for i, (k, m, a) in enumerate(inst):
+            b.init_uniform(i, airfoil_bcs(m, a)[0], cases.P_INF, cases.T_INF)
+        done, its, rat, st = b.run(0.8, 3000, tolerance=3e-2, check_every=10)
+        assert np.all(st == 1), st
+        assert len(set(its.tolist())) > 1          # they stop at different iterations
+        assert b.tuning() == (2048, 5)
+        got = [b.get_state(i) for i in range(len(inst))]
+    for i, (k, m, a) in enumerate(inst):
+        mach, bcs = airfoil_bcs(m, a)
+        c = cs[k]
+        c.init(mach, cases.P_INF, cases.T_INF)
+        c.run(bcs, 0.8, int(its[i]))
+        ref = c.fields()
+        for q in range(3):
+            assert np.array_equal(got[i][q], ref[q]), (i, q)
+    for c in cs:
+        c.close()
+
+
 def test_batch_instances_stop_at_their_own_tolerance(meshes):
     cs = [EulerCase(p) for p in meshes]
     inst = _instances()
