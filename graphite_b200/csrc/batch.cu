@@ -27,7 +27,6 @@ namespace gb {
 namespace {
 
 constexpr int kMaxRegions = 16;
-constexpr int kGhostTile = kBlock;
 
 struct InstDev {
     float* rho[2];
@@ -62,6 +61,46 @@ struct BcDev {
     float p, t;
 };
 
+// An instance's boundary conditions applied inside its gradient pass (the
+// Ghosts policy of grad_lim_cell over the batch's tables): ghost j of the
+// instance takes the condition of its region, computed by the thread of its
+// interior cell and stored into both value buffers.  On the one-layer
+// extruded meshes (about two ghosts per cell) this replaces a ghost kernel
+// that read the geometry and interior state of every ghost and wrote both
+// buffers, and the gradient pass's two gathers of each ghost state.
+struct BatchGhostBcs {
+    static constexpr bool kActive = true;
+    const uint8_t* region;     // per ghost (j - N)
+    const int* bc;             // per region: index into bcs, -1 none
+    const BcDev* bcs;
+    uint32_t N;
+    float* rho[2];
+    float4* rhou[2];
+    float* rhoe[2];
+    __device__ __forceinline__ bool state(uint32_t j, float3 nrm, float r1, float3 u1, float e1, float& r, float4& ru,
+                                          float& e) const {
+        const int b = bc[region[j - N]];
+        if (b < 0) return false;
+        const BcDev c = bcs[b];
+        if (c.type == 0) slip_state(nrm, r1, u1, e1, r, ru, e);
+        else farfield_state(nrm, r1, u1, e1, c.mach, c.p, c.t, r, ru, e);
+        return true;
+    }
+    __device__ __forceinline__ void store(uint32_t j, float r, float4 ru, float e) const {
+#pragma unroll
+        for (int k = 0; k < 2; ++k) {
+            rho[k][j] = r;
+            rhou[k][j] = ru;
+            rhoe[k][j] = e;
+        }
+    }
+};
+
+__device__ __forceinline__ BatchGhostBcs batch_ghosts(const InstDev& I, const MeshTab& M, const BcDev* bcs) {
+    return BatchGhostBcs{M.ghost_region, I.bc, bcs, M.m.N, {I.rho[0], I.rho[1]}, {I.rhou[0], I.rhou[1]},
+                         {I.rhoe[0], I.rhoe[1]}};
+}
+
 // Three forms of the batched gradient / flux kernels: variant 0 and 1 are
 // two register budgets (resident 256-thread blocks per SM; 1 trades a few
 // spills for one more resident block), variant 2 runs the gradient pass in
@@ -73,61 +112,38 @@ constexpr int kBatchVariants = 3;
 constexpr int kStagedThreads = 64;
 constexpr int kStagedBlocks = 14;
 
-__global__ void k_batch_bc(const int2* __restrict__ items, int n_items, InstDev* insts,
-                           const MeshTab* __restrict__ meshes, const BcDev* __restrict__ bcs) {
-    for (int it = blockIdx.x; it < n_items; it += gridDim.x) {
-        const int2 w = items[it];
-        const InstDev& I = insts[w.x];
-        if (I.status) continue;
-        const MeshTab& M = meshes[I.mesh];
-        const uint32_t g = (uint32_t)w.y * kGhostTile + threadIdx.x;
-        if (g >= M.G) continue;
-        const int b = I.bc[M.ghost_region[g]];
-        if (b < 0) continue;
-        const int cur = I.cur;
-        const BcDev bc = bcs[b];
-        float r, e;
-        float4 ru;
-        if (bc.type == 0)
-            slip_ghost(M.m.cell_geo, M.m.face_geo, M.ghost[g], I.rho[cur], I.rhou[cur], I.rhoe[cur], r, ru, e);
-        else
-            farfield_ghost(M.m.cell_geo, M.m.face_geo, M.ghost[g], I.rho[cur], I.rhou[cur], I.rhoe[cur], bc.mach,
-                           bc.p, bc.t, r, ru, e);
-        const uint32_t t = M.m.N + g;
-        for (int k = 0; k < 2; ++k) {
-            I.rho[k][t] = r;
-            I.rhou[k][t] = ru;
-            I.rhoe[k][t] = e;
-        }
-    }
-}
-
 template <bool TRANSPOSED, int BLOCKS>
 __global__ void __launch_bounds__(kBlock, BLOCKS)
-    k_batch_grad(const int2* __restrict__ items, const InstDev* insts, const MeshTab* __restrict__ meshes, int tile) {
+    k_batch_grad(const int2* __restrict__ items, const InstDev* insts, const MeshTab* __restrict__ meshes, int tile,
+                 const BcDev* __restrict__ bcs) {
     const int2 w = items[blockIdx.x];
     const InstDev& I = insts[w.x];
     if (I.status) return;
-    const MeshDev m = meshes[I.mesh].m;
+    const MeshTab& M = meshes[I.mesh];
+    const MeshDev m = M.m;
+    const BatchGhostBcs gh = batch_ghosts(I, M, bcs);
     const int cur = I.cur;
     const EulerState q{I.rho[cur], I.rhou[cur], I.rhoe[cur]};
     const EulerGrad g{nullptr, nullptr, nullptr, I.rec_rho, I.rec_rhou};
     const uint32_t c0 = (uint32_t)w.y * tile;
     const uint32_t c1 = min(m.N, c0 + (uint32_t)tile);
-    for (uint32_t i = c0 + threadIdx.x; i < c1; i += blockDim.x) grad_lim_cell<TRANSPOSED>(m, q, g, i);
+    for (uint32_t i = c0 + threadIdx.x; i < c1; i += blockDim.x)
+        grad_lim_cell<TRANSPOSED>(m, q, g, i, __ldg(&m.nfc[i]), EntriesGlobal{m, i}, gh);
 }
 
 template <bool TRANSPOSED>
 __global__ void __launch_bounds__(kStagedThreads, kStagedBlocks)
     k_batch_grad_staged(const int2* __restrict__ items, const InstDev* insts, const MeshTab* __restrict__ meshes,
-                        int tile) {
+                        int tile, const BcDev* __restrict__ bcs) {
     constexpr int B = kStagedThreads;
     __shared__ float4 s_dn[kSlots * B], s_df[kSlots * B];
     __shared__ uint32_t s_nbc[kSlots * B], s_twin[kSlots * B];
     const int2 w = items[blockIdx.x];
     const InstDev& I = insts[w.x];
     if (I.status) return;
-    const MeshDev m = meshes[I.mesh].m;
+    const MeshTab& M = meshes[I.mesh];
+    const MeshDev m = M.m;
+    const BatchGhostBcs gh = batch_ghosts(I, M, bcs);
     const int cur = I.cur;
     const EulerState q{I.rho[cur], I.rhou[cur], I.rhoe[cur]};
     const EulerGrad g{nullptr, nullptr, nullptr, I.rec_rho, I.rec_rhou};
@@ -146,7 +162,8 @@ __global__ void __launch_bounds__(kStagedThreads, kStagedBlocks)
             cp_async4(&s_twin[t * B + tid], &m.twin[k]);
         }
         asm volatile("cp.async.commit_group;\n" ::: "memory");
-        grad_lim_cell<TRANSPOSED>(m, q, g, i, nf, EntriesStaged<B>{s_nbc + tid, s_dn + tid, s_df + tid, s_twin + tid});
+        grad_lim_cell<TRANSPOSED>(m, q, g, i, nf, EntriesStaged<B>{s_nbc + tid, s_dn + tid, s_df + tid, s_twin + tid},
+                                  gh);
     }
 }
 
@@ -218,8 +235,6 @@ struct gbBatchImpl {
     int variant = 0;      // register budget of the gradient/flux kernels
     int2* d_cell_items = nullptr;
     int n_cell_items = 0;
-    int2* d_ghost_items = nullptr;
-    int n_ghost_items = 0;
     std::vector<void*> allocations;
     std::string signature;
 };
@@ -273,25 +288,13 @@ bool build_items(Batch* b) {
                 for (int i : insts) items.push_back(make_int2(i, (int)t));
         }
     }
-    std::vector<int2> gitems;
-    for (int i = 0; i < b->n_inst; ++i) {
-        if (!active(i)) continue;
-        const int64_t G = b->acc[b->h_inst[i].mesh].G;
-        for (int64_t t = 0; t * kGhostTile < G; ++t) gitems.push_back(make_int2(i, (int)t));
-    }
     if (b->d_cell_items) cudaFree(b->d_cell_items);
-    if (b->d_ghost_items) cudaFree(b->d_ghost_items);
     b->d_cell_items = nullptr;
-    b->d_ghost_items = nullptr;
     b->n_cell_items = (int)items.size();
-    b->n_ghost_items = (int)gitems.size();
-    if (!ok_(cudaMalloc((void**)&b->d_cell_items, std::max<size_t>(items.size(), 1) * sizeof(int2)), "batch items") ||
-        !ok_(cudaMalloc((void**)&b->d_ghost_items, std::max<size_t>(gitems.size(), 1) * sizeof(int2)), "batch items"))
+    if (!ok_(cudaMalloc((void**)&b->d_cell_items, std::max<size_t>(items.size(), 1) * sizeof(int2)), "batch items"))
         return false;
     cudaStream_t s = (cudaStream_t)gbGetStream();
     return ok_(cudaMemcpyAsync(b->d_cell_items, items.data(), items.size() * sizeof(int2), cudaMemcpyHostToDevice, s),
-               "batch items") &&
-           ok_(cudaMemcpyAsync(b->d_ghost_items, gitems.data(), gitems.size() * sizeof(int2), cudaMemcpyHostToDevice, s),
                "batch items");
 }
 
@@ -324,23 +327,21 @@ bool download_inst(Batch* b) {
 }
 
 void enqueue_iteration(Batch* b, float cfl, double tol, cudaStream_t s) {
-    const int gb_items = std::min(b->n_ghost_items, sm_count() * 8);
-    if (b->n_ghost_items)
-        k_batch_bc<<<gb_items, kGhostTile, 0, s>>>(b->d_ghost_items, b->n_ghost_items, b->d_inst, b->d_mesh, b->d_bcs);
+    // the boundary conditions are applied by the gradient kernels (BatchGhostBcs)
     if (b->n_cell_items) {
         const int n = b->n_cell_items;
         const bool tr = reference_momentum();
         if (b->variant == 0) {
-            if (tr) k_batch_grad<true, kBatchGradBlocks[0]><<<n, kBlock, 0, s>>>(b->d_cell_items, b->d_inst, b->d_mesh, b->tile);
-            else k_batch_grad<false, kBatchGradBlocks[0]><<<n, kBlock, 0, s>>>(b->d_cell_items, b->d_inst, b->d_mesh, b->tile);
+            if (tr) k_batch_grad<true, kBatchGradBlocks[0]><<<n, kBlock, 0, s>>>(b->d_cell_items, b->d_inst, b->d_mesh, b->tile, b->d_bcs);
+            else k_batch_grad<false, kBatchGradBlocks[0]><<<n, kBlock, 0, s>>>(b->d_cell_items, b->d_inst, b->d_mesh, b->tile, b->d_bcs);
             k_batch_flux<kBatchFluxBlocks[0]><<<n, kBlock, 0, s>>>(b->d_cell_items, b->d_inst, b->d_mesh, b->tile, cfl);
         } else if (b->variant == 1) {
-            if (tr) k_batch_grad<true, kBatchGradBlocks[1]><<<n, kBlock, 0, s>>>(b->d_cell_items, b->d_inst, b->d_mesh, b->tile);
-            else k_batch_grad<false, kBatchGradBlocks[1]><<<n, kBlock, 0, s>>>(b->d_cell_items, b->d_inst, b->d_mesh, b->tile);
+            if (tr) k_batch_grad<true, kBatchGradBlocks[1]><<<n, kBlock, 0, s>>>(b->d_cell_items, b->d_inst, b->d_mesh, b->tile, b->d_bcs);
+            else k_batch_grad<false, kBatchGradBlocks[1]><<<n, kBlock, 0, s>>>(b->d_cell_items, b->d_inst, b->d_mesh, b->tile, b->d_bcs);
             k_batch_flux<kBatchFluxBlocks[1]><<<n, kBlock, 0, s>>>(b->d_cell_items, b->d_inst, b->d_mesh, b->tile, cfl);
         } else {
-            if (tr) k_batch_grad_staged<true><<<n, kStagedThreads, 0, s>>>(b->d_cell_items, b->d_inst, b->d_mesh, b->tile);
-            else k_batch_grad_staged<false><<<n, kStagedThreads, 0, s>>>(b->d_cell_items, b->d_inst, b->d_mesh, b->tile);
+            if (tr) k_batch_grad_staged<true><<<n, kStagedThreads, 0, s>>>(b->d_cell_items, b->d_inst, b->d_mesh, b->tile, b->d_bcs);
+            else k_batch_grad_staged<false><<<n, kStagedThreads, 0, s>>>(b->d_cell_items, b->d_inst, b->d_mesh, b->tile, b->d_bcs);
             k_batch_flux<kBatchFluxBlocks[1]><<<n, kBlock, 0, s>>>(b->d_cell_items, b->d_inst, b->d_mesh, b->tile, cfl);
         }
     }
@@ -392,7 +393,7 @@ int64_t run_loop(Batch* b, float cfl, int64_t max_iter, double tol, int check_ev
     int active = b->n_inst;
     while (ok && done < max_iter) {
         const int64_t chunk = std::min<int64_t>(check_every, max_iter - done);
-        const int per_iter = 2 + (b->n_cell_items ? 2 : 0) - (b->n_ghost_items ? 0 : 1);
+        const int per_iter = 1 + (b->n_cell_items ? 2 : 0);
         for (int64_t i = 0; i < chunk && ok; ++i) {
             ok = ok_(cudaGraphLaunch(exec, s), "batch graph launch");
             count_launch(per_iter);
@@ -520,7 +521,6 @@ void gbBatchFree(gbBatch* b) {
     if (!b) return;
     for (void* p : b->allocations) cudaFree(p);
     if (b->d_cell_items) cudaFree(b->d_cell_items);
-    if (b->d_ghost_items) cudaFree(b->d_ghost_items);
     delete b;
 }
 

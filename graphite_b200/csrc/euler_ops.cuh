@@ -107,34 +107,37 @@ __device__ __forceinline__ void reconstruct(float r, float4 u, float e, float4 g
     ru = make_float3(u.x + du.x * gu[0].w, u.y + du.y * gu[1].w, u.z + du.z * gu[2].w);
 }
 
-// euler_slip_bc, src/models/euler.cu:412-442: the ghost of boundary face
-// gl = (interior cell, face) is the interior state with the normal momentum
-// mirrored (n outward from the interior cell).
+// euler_slip_bc, src/models/euler.cu:412-442: the ghost of a boundary face is
+// the interior state (r1, u, e1) with the normal momentum mirrored (n outward
+// from the interior cell).
+__device__ __forceinline__ void slip_state(float3 n, float r1, float3 u, float e1, float& r, float4& ru, float& e) {
+    r = r1;
+    e = e1;
+    const float3 ug = u - n * (2.f * dot(n, u));
+    ru = make_float4(ug.x, ug.y, ug.z, 0.f);
+}
+
+// The outward normal of boundary face gl = (interior cell, face); the same
+// arithmetic as the per-entry normals of entry_geo_cell.
+__device__ __forceinline__ float3 ghost_normal(const float4* __restrict__ cell_geo,
+                                               const float4* __restrict__ face_geo, uint2 gl) {
+    return outer_normal(f3(face_geo[2 * gl.y]), f3(face_geo[2 * gl.y + 1]) - f3(cell_geo[gl.x]));
+}
+
 __device__ __forceinline__ void slip_ghost(const float4* __restrict__ cell_geo, const float4* __restrict__ face_geo,
                                            uint2 gl, const float* rho, const float4* rhou, const float* rhoe,
                                            float& r, float4& ru, float& e) {
     const uint32_t c1 = gl.x;
-    const float3 n = outer_normal(f3(face_geo[2 * gl.y]), f3(face_geo[2 * gl.y + 1]) - f3(cell_geo[c1]));
-    r = rho[c1];
-    const float3 u = f3(rhou[c1]);
-    e = rhoe[c1];
-    const float3 ug = u - n * (2.f * dot(n, u));
-    ru = make_float4(ug.x, ug.y, ug.z, 0.f);
+    slip_state(ghost_normal(cell_geo, face_geo, gl), rho[c1], f3(rhou[c1]), rhoe[c1], r, ru, e);
 }
 
 // euler_inletoutlet_bc, src/models/euler.cu:446-520 (gamma = 1.4, R = 1):
 // inflow (u.n < 0) supersonic -> free stream, subsonic -> interior pressure
 // with free-stream temperature and Mach; outflow supersonic -> interior,
 // subsonic -> free-stream pressure with interior temperature and velocity.
-__device__ __forceinline__ void farfield_ghost(const float4* __restrict__ cell_geo,
-                                               const float4* __restrict__ face_geo, uint2 gl, const float* rho,
-                                               const float4* rhou, const float* rhoe, float3 imach, float ip,
+// (r1, ru1, e1) is the interior state, n the outward normal.
+__device__ __forceinline__ void farfield_state(float3 n, float r1, float3 ru1, float e1, float3 imach, float ip,
                                                float it, float& r, float4& ru4, float& e) {
-    const uint32_t c1 = gl.x;
-    const float3 n = outer_normal(f3(face_geo[2 * gl.y]), f3(face_geo[2 * gl.y + 1]) - f3(cell_geo[c1]));
-    const float r1 = rho[c1];
-    const float3 ru1 = f3(rhou[c1]);
-    const float e1 = rhoe[c1];
     const float3 u = ru1 * (1.f / r1);
     const float p = 0.4f * (e1 - 0.5f / r1 * dot(ru1, ru1));
     const float tt = p / r1;
@@ -166,6 +169,29 @@ __device__ __forceinline__ void farfield_ghost(const float4* __restrict__ cell_g
     }
     ru4 = make_float4(ru.x, ru.y, ru.z, 0.f);
 }
+
+__device__ __forceinline__ void farfield_ghost(const float4* __restrict__ cell_geo,
+                                               const float4* __restrict__ face_geo, uint2 gl, const float* rho,
+                                               const float4* rhou, const float* rhoe, float3 imach, float ip,
+                                               float it, float& r, float4& ru4, float& e) {
+    const uint32_t c1 = gl.x;
+    farfield_state(ghost_normal(cell_geo, face_geo, gl), rho[c1], f3(rhou[c1]), rhoe[c1], imach, ip, it, r, ru4, e);
+}
+
+// A Ghosts policy of grad_lim_cell applies boundary conditions inside the
+// gradient pass instead of by a separate ghost kernel: with kActive,
+// state(j, n, interior state) gives the state of ghost j when a condition
+// covers it (slip_state / farfield_state with the entry's outward normal,
+// which is bitwise the normal the ghost kernels compute) and store() writes
+// it into both value buffers.  NoGhostBcs leaves every ghost to its stored
+// state.
+struct NoGhostBcs {
+    static constexpr bool kActive = false;
+    __device__ __forceinline__ bool state(uint32_t, float3, float, float3, float, float&, float4&, float&) const {
+        return false;
+    }
+    __device__ __forceinline__ void store(uint32_t, float, float4, float) const {}
+};
 
 // Per-face entry data of cell i (slot t = 0..nf-1), read straight from the
 // slot-major arrays at entry i + t N.
@@ -212,9 +238,9 @@ __device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
 // each ghost neighbour, which carries this cell's gradient and limiter
 // (fvmScalGradLimBc / fvmVecGradLimBc, src/fvmops.cu:272-304).  nf is the
 // cell's face count; e supplies its entries.
-template <bool TRANSPOSED, typename Entries>
+template <bool TRANSPOSED, typename Entries, typename Ghosts = NoGhostBcs>
 __device__ __forceinline__ void grad_lim_cell(const MeshDev& m, EulerState q, EulerGrad g, uint32_t i, uint32_t nf,
-                                              const Entries& e) {
+                                              const Entries& e, const Ghosts& gh = Ghosts()) {
     float v[5];
     float4 u0;
     {
@@ -230,8 +256,15 @@ __device__ __forceinline__ void grad_lim_cell(const MeshDev& m, EulerState q, Eu
         const uint32_t j = e.nbc(t);
         const float4 dw = e.dn(t);                   // (c_j - c_i, 1 / |c_j - c_i|^2)
         const float3 d = f3(dw);
-        const float4 uj = __ldg(&q.rhou[j]);
-        const float vj[5] = {__ldg(&q.rho[j]), uj.x, uj.y, uj.z, __ldg(&q.rhoe[j])};
+        float rj, ej;
+        float4 uj;
+        if (!(Ghosts::kActive && j >= m.N &&
+              gh.state(j, f3(__ldg(&m.cf_geo[i + t * m.N])), v[0], f3(u0), v[4], rj, uj, ej))) {
+            uj = __ldg(&q.rhou[j]);
+            rj = __ldg(&q.rho[j]);
+            ej = __ldg(&q.rhoe[j]);
+        }
+        const float vj[5] = {rj, uj.x, uj.y, uj.z, ej};
 #pragma unroll
         for (int c = 0; c < 5; ++c) {
             gs[c] = gs[c] + (d * (vj[c] - v[c])) * dw.w;
@@ -272,8 +305,16 @@ __device__ __forceinline__ void grad_lim_cell(const MeshDev& m, EulerState q, Eu
             // ghost neighbour: its state with this cell's gradient and limiter
             const uint32_t j = m.N + (tw - m.S);
             const float3 fc = f3(__ldg(&m.face_geo[2 * __ldg(&m.nb[k]).x + 1]));
-            reconstruct<TRANSPOSED>(__ldg(&q.rho[j]), __ldg(&q.rhou[j]), __ldg(&q.rhoe[j]), gr, gu, ge,
-                                    fc - f3(__ldg(&m.cell_geo[j])), rr, ru, re);
+            float rj, ej;
+            float4 uj;
+            if (Ghosts::kActive && gh.state(j, f3(__ldg(&m.cf_geo[k])), v[0], f3(u0), v[4], rj, uj, ej)) {
+                gh.store(j, rj, uj, ej);
+            } else {
+                uj = __ldg(&q.rhou[j]);
+                rj = __ldg(&q.rho[j]);
+                ej = __ldg(&q.rhoe[j]);
+            }
+            reconstruct<TRANSPOSED>(rj, uj, ej, gr, gu, ge, fc - f3(__ldg(&m.cell_geo[j])), rr, ru, re);
             g.rec_rho[tw] = rr;
             g.rec_rhou[tw] = make_float4(ru.x, ru.y, ru.z, re);
         }

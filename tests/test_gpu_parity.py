@@ -156,17 +156,24 @@ def test_channel_2000_iterations_match_reference(su2_paths):
             assert d.max() < 1e-3 and d.mean() < 5e-5, (key, d.max(), d.mean())
 
 
-def test_graph_run_is_bitwise_the_per_call_loop(su2_paths):
+# every region; one region left without a condition (its ghosts keep their
+# stored state); a region given two conditions (the later one holds)
+BC_SETS = {"all": BCS, "no_sides": [b for b in BCS if b[1] != "sides"],
+           "upper_twice": BCS + [("farfield", "upper") + tuple(cases.CHANNEL_MACH) + (cases.P_INF, cases.T_INF)]}
+
+
+@pytest.mark.parametrize("bcs", list(BC_SETS))
+def test_graph_run_is_bitwise_the_per_call_loop(bcs, su2_paths):
     """gbEulerRun (replayed CUDA graphs) computes exactly what the per-call
-    loop computes."""
+    loop computes, ghost values included, whichever regions have conditions."""
     hs, fs = [], []
     for mode in ("calls", "graph"):
         with EulerCase(su2_paths("tet_12x6x2")) as c:
             c.init(*INIT)
             if mode == "calls":
-                h = np.array([c.iterate(BCS, 0.8) for _ in range(57)])
+                h = np.array([c.iterate(BC_SETS[bcs], 0.8) for _ in range(57)])
             else:
-                h = c.run(BCS, 0.8, 57)
+                h = c.run(BC_SETS[bcs], 0.8, 57)
             hs.append(h)
             fs.append(c.fields())
     assert np.array_equal(hs[0].astype(np.float32), hs[1].astype(np.float32))
