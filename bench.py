@@ -549,9 +549,9 @@ def run_warm_start(args, dev_stream):
     t0 = clock()
     ws = WarmStart(c, wall="wing", seed=WARM_SEED)
     with EulerBatch([c], [(0, airfoil_case(m, a)[1]) for m, a in train]) as b:
-        b.autotune(cfl, trial_iters=3)
         for i, (m, a) in enumerate(train):
             b.init_uniform(i, airfoil_case(m, a)[0], P_INF, T_INF)
+        b.autotune(cfl, trial_iters=3)       # trials run from these states, which it restores
         _, gen_its, _, gen_st = b.run(cfl, cap, tolerance=tol, check_every=200)
         for i, (m, a) in enumerate(train):
             if gen_st[i] == 1:
@@ -582,6 +582,8 @@ def run_warm_start(args, dev_stream):
     # 4. batched cold / batched warm
     spec = [(0, airfoil_case(m, a)[1]) for m, a in held]
     with EulerBatch([c], spec) as b:
+        for i, (mv, p, t) in enumerate(cases):
+            b.init_uniform(i, mv, p, t)
         b.autotune(cfl, trial_iters=3)
         t0 = clock()
         cold_its, _, cold_st, _ = solve_warm(b, [None] * len(held), cases, cfl, cap, tol)

@@ -631,37 +631,47 @@ int gbBatchAutotune(gbBatch* b, gb_scalar cfl, int trial_iters, int* tile_out, i
         cudaEventCreate(&e1);
         float best = 1e30f;
         Tuning best_t{b->tile, b->schedule, b->variant};
+        // every candidate timed over trial_iters iterations, then the 4
+        // fastest again over 4 x trial_iters: the short trials only rank
+        // the field, the longer ones decide between close candidates
         const int tiles[] = {256, 512, 1024, 2048};
-        for (int var = 0; var < kBatchVariants && ok; ++var)
-        for (int sched = 0; sched < 2 && ok; ++sched) {
-            for (int tile : tiles) {
-                if (!ok) break;
-                b->h_inst = base;
-                b->tile = tile;
-                b->schedule = sched;
-                b->variant = var;
-                reset_counters(b, 1 << 30, false);
-                ok = size_partials(b) && build_items(b) && upload_inst(b);
-                // one untimed iteration, then the timed trial
-                if (ok) enqueue_iteration(b, cfl, 0.0, s);
-                cudaEventRecord(e0, s);
-                for (int it = 0; it < trial_iters && ok; ++it) enqueue_iteration(b, cfl, 0.0, s);
-                cudaEventRecord(e1, s);
-                ok = ok && ok_(cudaEventSynchronize(e1), "gbBatchAutotune");
-                float ms = 0.f;
-                cudaEventElapsedTime(&ms, e0, e1);
-                if (ok && ms < best) { best = ms; best_t = Tuning{tile, sched, var}; }
-                // restore the states
-                for (int i = 0; i < b->n_inst && ok; ++i) {
-                    const InstDev& I = base[i];
-                    const MeshAccess& A = b->acc[I.mesh];
-                    const int64_t NG = A.N + A.G;
-                    for (int k = 0; k < 2 && ok; ++k)
-                        ok = ok_(cudaMemcpyAsync(I.rho[k], saved[i][0], NG * 4, cudaMemcpyDeviceToDevice, s), "restore") &&
-                             ok_(cudaMemcpyAsync(I.rhou[k], saved[i][1], NG * 16, cudaMemcpyDeviceToDevice, s), "restore") &&
-                             ok_(cudaMemcpyAsync(I.rhoe[k], saved[i][2], NG * 4, cudaMemcpyDeviceToDevice, s), "restore");
-                }
+        std::vector<Tuning> cands;
+        for (int var = 0; var < kBatchVariants; ++var)
+            for (int sched = 0; sched < 2; ++sched)
+                for (int tile : tiles) cands.push_back(Tuning{tile, sched, var});
+        auto trial = [&](const Tuning& c, int iters) -> float {
+            b->h_inst = base;
+            b->tile = c.tile;
+            b->schedule = c.schedule;
+            b->variant = c.variant;
+            reset_counters(b, 1 << 30, false);
+            ok = ok && size_partials(b) && build_items(b) && upload_inst(b);
+            // one untimed iteration, then the timed trial
+            if (ok) enqueue_iteration(b, cfl, 0.0, s);
+            cudaEventRecord(e0, s);
+            for (int it = 0; it < iters && ok; ++it) enqueue_iteration(b, cfl, 0.0, s);
+            cudaEventRecord(e1, s);
+            ok = ok && ok_(cudaEventSynchronize(e1), "gbBatchAutotune");
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, e0, e1);
+            // restore the states
+            for (int i = 0; i < b->n_inst && ok; ++i) {
+                const InstDev& I = base[i];
+                const MeshAccess& A = b->acc[I.mesh];
+                const int64_t NG = A.N + A.G;
+                for (int k = 0; k < 2 && ok; ++k)
+                    ok = ok_(cudaMemcpyAsync(I.rho[k], saved[i][0], NG * 4, cudaMemcpyDeviceToDevice, s), "restore") &&
+                         ok_(cudaMemcpyAsync(I.rhou[k], saved[i][1], NG * 16, cudaMemcpyDeviceToDevice, s), "restore") &&
+                         ok_(cudaMemcpyAsync(I.rhoe[k], saved[i][2], NG * 4, cudaMemcpyDeviceToDevice, s), "restore");
             }
+            return ms;
+        };
+        std::vector<std::pair<float, size_t>> first;
+        for (size_t c = 0; c < cands.size() && ok; ++c) first.push_back({trial(cands[c], trial_iters), c});
+        std::sort(first.begin(), first.end());
+        for (size_t k = 0; k < std::min<size_t>(4, first.size()) && ok; ++k) {
+            const float ms = trial(cands[first[k].second], 4 * trial_iters);
+            if (ok && ms < best) { best = ms; best_t = cands[first[k].second]; }
         }
         cudaEventDestroy(e0);
         cudaEventDestroy(e1);

@@ -288,8 +288,9 @@ int gbBatchSetTuning(gbBatch* batch, int tile_cells, int schedule);
 int gbBatchGetTuning(gbBatch* batch, int* tile_cells, int* schedule);
 
 /* Times trial_iters iterations of every (tile, schedule) candidate from the
- * current states (restored afterwards) and keeps the fastest; results are
- * cached per (mesh sizes, instances per mesh) for the process. */
+ * current states (restored afterwards), then the 4 fastest again over
+ * 4 x trial_iters, and keeps the fastest of those; results are cached per
+ * (mesh sizes, instances per mesh) for the process. */
 int gbBatchAutotune(gbBatch* batch, gb_scalar cfl, int trial_iters, int* tile_cells, int* schedule);
 
 /* Runs until every instance has converged (residual / first residual <

@@ -98,10 +98,14 @@ def test_batch_instances_stop_at_their_own_tolerance(meshes):
     inst = _instances()
     spec = [(k, airfoil_bcs(m, a)[1]) for k, m, a in inst]
     with EulerBatch(cs, spec) as b:
-        tile, sched = b.autotune(0.8, trial_iters=3)
-        assert tile % 256 == 0 and sched in range(6)
         for i, (k, m, a) in enumerate(inst):
             b.init_uniform(i, airfoil_bcs(m, a)[0], cases.P_INF, cases.T_INF)
+        before = [b.get_state(i) for i in range(len(inst))]
+        tile, sched = b.autotune(0.8, trial_iters=3)
+        assert tile % 256 == 0 and sched in range(6)
+        for i in range(len(inst)):                 # the trials' iterations are undone
+            for q in range(3):
+                assert np.array_equal(b.get_state(i)[q], before[i][q])
         done, its, rat, st, hist = b.run(0.8, 3000, tolerance=1e-2, check_every=50, history=True)
         assert np.all(st == 1), st
         assert np.all(rat < 1e-2)
