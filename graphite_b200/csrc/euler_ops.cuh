@@ -45,14 +45,15 @@ __device__ __forceinline__ float3 sym_mul(float4 l0, float4 l1, float3 g) {
 // limiter(), src/fvmops.cu:118-169: smoothed switch on (max-min)^2 against
 // (K |d|)^3 with K = 1, Michalak function y - y^2/4 (y < 2), scaled by 0.8.
 // k3 = |d|^3 is shared by the five variables of a face.
+// Where sig = 1 the blend sig + (1 - sig) lim is exactly 1 for the finite
+// lim this function forms, so that case returns before lim is computed.
 __device__ __forceinline__ float limiter(float u, float3 g, float umin, float umax, float3 d, float k3) {
-    const float delta = dot(g, d);
     const float du = umax - u, dd = umin - u;
     const float dmm2 = (du - dd) * (du - dd);
+    if (dmm2 <= k3) return 1.f;
+    const float delta = dot(g, d);
     float sig;
-    if (dmm2 <= k3) {
-        sig = 1.f;
-    } else if (dmm2 <= 2.f * k3) {
+    if (dmm2 <= 2.f * k3) {
         const float y = dmm2 / k3 - 1.f;
         sig = 2.f * y * y * y - 3.f * y * y + 1.f;
     } else {
