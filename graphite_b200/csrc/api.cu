@@ -849,7 +849,7 @@ void launch_nsi_init(int64_t n, float* p, float4* u, float p0, float3 u0, cudaSt
 void launch_nsi_bc(const DevMesh& m, uint32_t g0, uint32_t g1, int type, float* p[2], float4* u[2], int cur,
                    float3 vinf, float pinf, cudaStream_t s);
 void launch_nsi_grad(const DevMesh& m, const float* p, const float4* u, float4* gp, float4* gu, int limited,
-                     cudaStream_t s);
+                     cudaStream_t s, const NsiGhostTable* ghosts = nullptr);
 void launch_nsi_flux(const DevMesh& m, const float* p, const float4* u, const float4* gp, const float4* gu, float* p_n,
                      float4* u_n, float* err, double* partials, float cfl, float nu, float beta2, int corrected,
                      cudaStream_t s);
@@ -895,11 +895,11 @@ void enqueue_nsi_bc(cuMesh* mesh, FvmField* velocity, FvmField* pressure, int r,
 }
 
 void enqueue_nsi_step(cuMesh* mesh, FvmField* velocity, FvmField* pressure, FvmField* error, float cfl, int cur,
-                      cudaStream_t s) {
+                      cudaStream_t s, const NsiGhostTable* ghosts = nullptr) {
     MeshImpl* mi = impl(mesh);
     FieldImpl *vi = impl(velocity), *pi = impl(pressure), *ei = impl(error);
     launch_nsi_grad(mi->dev, (const float*)pi->val[cur], (const float4*)vi->val[cur], pi->grad, vi->grad,
-                    t_nsi.limited, s);
+                    t_nsi.limited, s, ghosts);
     launch_nsi_flux(mi->dev, (const float*)pi->val[cur], (const float4*)vi->val[cur], pi->grad, vi->grad,
                     (float*)pi->val[1 - cur], (float4*)vi->val[1 - cur], (float*)ei->val[ei->cur], ei->partials, cfl,
                     (float)t_nsi.viscosity, (float)(t_nsi.beta * t_nsi.beta), t_nsi.corrected, s);
@@ -1021,6 +1021,28 @@ int64_t gbNSIRun(cuMesh* mesh, FvmField* velocity, FvmField* pressure, FvmField*
         return -1;
     }
     double* out = mi->dev.red + mi->dev.n_red_max;
+    // On ghost-heavy meshes (one-layer extrusions carry two span ghosts per
+    // cell) the gradient kernel applies the boundary conditions itself
+    // (NsiGhostTable); on the others the ghost kernels cost less than the
+    // extra work in the gradient pass.
+    const int n_regions = (int)mi->topo.regions.size();
+    const bool inline_bcs = n_regions > 0 && n_regions <= kMaxNsiRegions && 4 * mi->dev.G >= mi->dev.N;
+    NsiGhostTable gt{};
+    if (inline_bcs) {
+        gt.n = n_regions;
+        for (int r = 0; r <= n_regions; ++r) gt.start[r] = mi->num.region_start[r];
+        for (int r = 0; r < n_regions; ++r) gt.type[r] = -1;
+        for (int b = 0; b < n_bc; ++b) {   // a later condition on the same region replaces an earlier one
+            const int r = (int)bcs[b].region_id;
+            gt.type[r] = bcs[b].type == 1 ? 1 : (bcs[b].type == 2 ? 2 : 0);
+            gt.vinf[r] = make_float3(bcs[b].mach.x, bcs[b].mach.y, bcs[b].mach.z);
+            gt.pinf[r] = bcs[b].pressure;
+        }
+        for (int k = 0; k < 2; ++k) {
+            gt.p[k] = (float*)impl(pressure)->val[k];
+            gt.u[k] = (float4*)impl(velocity)->val[k];
+        }
+    }
     cudaGraphExec_t exec[2] = {nullptr, nullptr};
     cudaStream_t cap = nullptr;
     bool ok = cuda_ok(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking), "gbNSIRun");
@@ -1029,18 +1051,18 @@ int64_t gbNSIRun(cuMesh* mesh, FvmField* velocity, FvmField* pressure, FvmField*
         cudaGraph_t g = nullptr;
         ok = cuda_ok(cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal), "graph capture");
         if (!ok) break;
-        for (int b = 0; b < n_bc; ++b) {
+        for (int b = 0; b < n_bc && !inline_bcs; ++b) {
             const int type = bcs[b].type == 1 ? 1 : (bcs[b].type == 2 ? 2 : 0);
             enqueue_nsi_bc(mesh, velocity, pressure, (int)bcs[b].region_id, type, k, bcs[b].mach, bcs[b].pressure, cap);
         }
-        enqueue_nsi_step(mesh, velocity, pressure, error, cfl, k, cap);
+        enqueue_nsi_step(mesh, velocity, pressure, error, cfl, k, cap, inline_bcs ? &gt : nullptr);
         launch_reduce_final(nb, ei->partials, out, d_hist, d_counter, cap);
         ok = cuda_ok(cudaStreamEndCapture(cap, &g), "graph capture") &&
              cuda_ok(cudaGraphInstantiate(&exec[k], g, 0), "graph instantiate");
         if (g) cudaGraphDestroy(g);
     }
     t_counting = true;
-    const int per_iter = n_bc + 3;
+    const int per_iter = (inline_bcs ? 0 : n_bc) + 3;
     int cur = impl(pressure)->cur;
     int64_t done = 0;
     std::vector<double> hist((size_t)n_iter, 0.0);

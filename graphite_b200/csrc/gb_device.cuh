@@ -104,6 +104,22 @@ void launch_bc_farfield(const DevMesh& m, uint32_t g0, uint32_t g1, float* rho[2
                         float* rhoe[2], int cur, float3 mach, float p, float t, cudaStream_t s);
 void launch_entry_geo(const DevMesh& m, cudaStream_t s);
 void launch_grad_lim(const DevMesh& m, EulerState q, EulerGrad g, bool transposed, cudaStream_t s);
+
+// Boundary conditions of the incompressible path applied by its gradient
+// kernel, by ghost region: ghosts [start[r], start[r+1]) (absolute cell
+// indices) get type[r]: -1 none (their stored state), 0 slip, 1 inlet/outlet
+// with vinf[r], pinf[r], 2 no-slip wall; the computed ghost states are stored
+// into both value buffers p[], u[].
+constexpr int kMaxNsiRegions = 16;
+struct NsiGhostTable {
+    int n;
+    uint32_t start[kMaxNsiRegions + 1];
+    int type[kMaxNsiRegions];
+    float3 vinf[kMaxNsiRegions];
+    float pinf[kMaxNsiRegions];
+    float* p[2];
+    float4* u[2];
+};
 void launch_flux(const DevMesh& m, EulerState q, FaceRecs r, float* rho_n, float4* rhou_n, float* rhoe_n,
                  float* err, double* partials, float cfl, cudaStream_t s);
 void launch_reduce_partials(int64_t n, const float* v, double* partials, cudaStream_t s);

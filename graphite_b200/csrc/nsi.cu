@@ -39,20 +39,10 @@ __global__ void k_nsi_init(int64_t n, float* p, float4* u, float p0, float3 u0) 
 // pressure), 2 no-slip wall (velocity mirrored through zero).  The pressure
 // is extrapolated from the interior except at outflow.  Both value buffers
 // are written.
-__global__ void k_nsi_bc(uint32_t g0, uint32_t g1, uint32_t N, const float4* __restrict__ cell_geo,
-                         const float4* __restrict__ face_geo, const uint2* __restrict__ ghost, float* pa, float* pb,
-                         float4* ua, float4* ub, int cur, int type, float3 vinf, float pinf) {
-    const uint32_t t = g0 + blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= g1) return;
-    const uint2 gl = ghost[t - N];
-    const uint32_t c1 = gl.x;
-    const float3 n = outer_normal(f3(face_geo[2 * gl.y]), f3(face_geo[2 * gl.y + 1]) - f3(cell_geo[c1]));
-    const float* p = cur ? pb : pa;
-    const float4* u = cur ? ub : ua;
-    const float pi = p[c1];
-    const float3 ui = f3(u[c1]);
-    float pg;
-    float3 ug;
+// The ghost state of one boundary face from its interior state (pi, ui) and
+// outward normal n.
+__device__ __forceinline__ void nsi_ghost_state(int type, float3 n, float pi, float3 ui, float3 vinf, float pinf,
+                                                float& pg, float3& ug) {
     if (type == 0) {
         ug = ui - n * (2.f * dot(n, ui));
         pg = pi;
@@ -66,6 +56,21 @@ __global__ void k_nsi_bc(uint32_t g0, uint32_t g1, uint32_t N, const float4* __r
         ug = ui;
         pg = pinf;
     }
+}
+
+__global__ void k_nsi_bc(uint32_t g0, uint32_t g1, uint32_t N, const float4* __restrict__ cell_geo,
+                         const float4* __restrict__ face_geo, const uint2* __restrict__ ghost, float* pa, float* pb,
+                         float4* ua, float4* ub, int cur, int type, float3 vinf, float pinf) {
+    const uint32_t t = g0 + blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= g1) return;
+    const uint2 gl = ghost[t - N];
+    const uint32_t c1 = gl.x;
+    const float3 n = outer_normal(f3(face_geo[2 * gl.y]), f3(face_geo[2 * gl.y + 1]) - f3(cell_geo[c1]));
+    const float* p = cur ? pb : pa;
+    const float4* u = cur ? ub : ua;
+    float pg;
+    float3 ug;
+    nsi_ghost_state(type, n, p[c1], f3(u[c1]), vinf, pinf, pg, ug);
     const float4 u4 = make_float4(ug.x, ug.y, ug.z, 0.f);
     pa[t] = pg;
     pb[t] = pg;
@@ -76,9 +81,14 @@ __global__ void k_nsi_bc(uint32_t g0, uint32_t g1, uint32_t N, const float4* __r
 // Least-squares gradients of p, u_x, u_y, u_z (src/fvmops.cu:51-111 on the
 // per-entry geometry) and, when `limited`, the reference's limiters
 // (src/fvmops.cu:175-266); otherwise the limiter is 1 (unlimited second order).
+// With GHOSTS the boundary conditions of gh are applied here: the thread of a
+// ghost's interior cell computes the ghost's state (nsi_ghost_state with the
+// entry's outward normal, bitwise the normal k_nsi_bc computes), uses it and
+// stores it into both value buffers, for the flux pass and the caller.
+template <bool GHOSTS>
 __global__ void __launch_bounds__(kBlock, kNsiBlocks)
     k_nsi_grad(MeshDev m, const float* __restrict__ p, const float4* __restrict__ u, float4* gp, float4* gu,
-               int limited) {
+               int limited, NsiGhostTable gh) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= m.N) return;
     float v[4];
@@ -96,8 +106,30 @@ __global__ void __launch_bounds__(kBlock, kNsiBlocks)
         const uint32_t j = __ldg(&m.nbc[k]);
         const float4 dw = __ldg(&m.dn[k]);
         const float3 d = f3(dw);
-        const float4 uj = __ldg(&u[j]);
-        const float vj[4] = {__ldg(&p[j]), uj.x, uj.y, uj.z};
+        float vj[4];
+        bool computed = false;
+        if (GHOSTS && j >= m.N) {
+            int r = 0;
+            while (r < gh.n - 1 && j >= gh.start[r + 1]) ++r;
+            if (gh.type[r] >= 0) {
+                float pg;
+                float3 ug;
+                nsi_ghost_state(gh.type[r], f3(__ldg(&m.cf_geo[k])), v[0], make_float3(v[1], v[2], v[3]),
+                                gh.vinf[r], gh.pinf[r], pg, ug);
+                const float4 u4 = make_float4(ug.x, ug.y, ug.z, 0.f);
+#pragma unroll
+                for (int b = 0; b < 2; ++b) {
+                    gh.p[b][j] = pg;
+                    gh.u[b][j] = u4;
+                }
+                vj[0] = pg; vj[1] = ug.x; vj[2] = ug.y; vj[3] = ug.z;
+                computed = true;
+            }
+        }
+        if (!computed) {
+            const float4 uj = __ldg(&u[j]);
+            vj[0] = __ldg(&p[j]); vj[1] = uj.x; vj[2] = uj.y; vj[3] = uj.z;
+        }
 #pragma unroll
         for (int c = 0; c < 4; ++c) {
             gs[c] = gs[c] + (d * (vj[c] - v[c])) * dw.w;
@@ -272,9 +304,10 @@ void launch_nsi_bc(const DevMesh& m, uint32_t g0, uint32_t g1, int type, float* 
 }
 
 void launch_nsi_grad(const DevMesh& m, const float* p, const float4* u, float4* gp, float4* gu, int limited,
-                     cudaStream_t s) {
+                     cudaStream_t s, const NsiGhostTable* ghosts) {
     if (m.N == 0) return;
-    k_nsi_grad<<<grid_of(m.N), kBlock, 0, s>>>(mesh_dev(m), p, u, gp, gu, limited);
+    if (ghosts) k_nsi_grad<true><<<grid_of(m.N), kBlock, 0, s>>>(mesh_dev(m), p, u, gp, gu, limited, *ghosts);
+    else k_nsi_grad<false><<<grid_of(m.N), kBlock, 0, s>>>(mesh_dev(m), p, u, gp, gu, limited, NsiGhostTable{});
     count_launch();
 }
 

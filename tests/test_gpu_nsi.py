@@ -49,21 +49,32 @@ def test_nsi_matches_fp64_oracle(cyl, corrected, limited):
         NSICase.set_constants()
 
 
-def test_nsi_per_call_loop_equals_graph(cyl):
-    """The per-call loop (BCs, FvmNSIStepPrepare, FvmNSIStep, residual) and the
-    replayed graphs give the same bits."""
+# every region; the span sides left without a condition (their ghosts keep
+# their stored state); the sides given two conditions (the later one holds)
+NSI_BC_SETS = {"all": BCS, "no_sides": BCS[:2], "sides_twice": BCS + [("wall", "sides")]}
+
+
+@pytest.mark.parametrize("bcs,limited", [("all", False), ("all", True), ("no_sides", False), ("sides_twice", False)])
+def test_nsi_per_call_loop_equals_graph(cyl, bcs, limited):
+    """The per-call loop (BC kernels, FvmNSIStepPrepare, FvmNSIStep, residual)
+    and the replayed graphs (on this one-layer mesh the gradient kernel applies
+    the boundary conditions) give the same bits, ghost values included."""
     _, path = cyl
-    a, b = NSICase(path), NSICase(path)
-    for c in (a, b):
-        c.init((1.0, 0.0, 0.0), 0.0)
-    h = a.run(BCS, 0.5, 40)
-    h2 = np.array([b.iterate(BCS, 0.5) for _ in range(40)])
-    ua, pa = a.fields()
-    ub, pb = b.fields()
-    assert np.array_equal(ua, ub) and np.array_equal(pa, pb)
-    np.testing.assert_allclose(h, h2, rtol=1e-6)
-    a.close()
-    b.close()
+    NSICase.set_constants(1.0, 0.025, 2.0, True, limited)
+    try:
+        a, b = NSICase(path), NSICase(path)
+        for c in (a, b):
+            c.init((1.0, 0.0, 0.0), 0.0)
+        h = a.run(NSI_BC_SETS[bcs], 0.5, 40)
+        h2 = np.array([b.iterate(NSI_BC_SETS[bcs], 0.5) for _ in range(40)])
+        ua, pa = a.fields()
+        ub, pb = b.fields()
+        assert np.array_equal(ua, ub) and np.array_equal(pa, pb)
+        np.testing.assert_allclose(h, h2, rtol=1e-6)
+        a.close()
+        b.close()
+    finally:
+        NSICase.set_constants()
 
 
 def test_nsi_bad_calls_are_rejected(cyl):
