@@ -772,6 +772,30 @@ int64_t gbEulerRun(cuMesh* mesh, FvmField* rho, FvmField* rhou, FvmField* rhoe, 
         return -1;
     }
     double* out = mi->dev.red + mi->dev.n_red_max;
+    // On ghost-heavy meshes (one-layer extrusions carry two span ghosts per
+    // cell) the gradient kernel applies the boundary conditions itself
+    // (GhostBcTable); on the others the ghost kernels cost less than the
+    // extra work in the gradient pass.
+    const int n_regions = (int)mi->topo.regions.size();
+    const bool inline_bcs = n_regions > 0 && n_regions <= kMaxBcRegions && 4 * mi->dev.G >= mi->dev.N;
+    GhostBcTable gbt{};
+    if (inline_bcs) {
+        gbt.n = n_regions;
+        for (int r = 0; r <= n_regions; ++r) gbt.start[r] = mi->num.region_start[r];
+        for (int r = 0; r < n_regions; ++r) gbt.type[r] = -1;
+        for (int b = 0; b < n_bc; ++b) {   // a later condition on the same region replaces an earlier one
+            const int r = (int)bcs[b].region_id;
+            gbt.type[r] = bcs[b].type;
+            gbt.mach[r] = make_float3(bcs[b].mach.x, bcs[b].mach.y, bcs[b].mach.z);
+            gbt.p[r] = bcs[b].pressure;
+            gbt.temp[r] = bcs[b].temperature;
+        }
+        for (int k = 0; k < 2; ++k) {
+            gbt.rho[k] = (float*)impl(rho)->val[k];
+            gbt.rhou[k] = (float4*)impl(rhou)->val[k];
+            gbt.rhoe[k] = (float*)impl(rhoe)->val[k];
+        }
+    }
     // one graph per value buffer parity: BCs, gradients+limiters, flux+update, residual
     cudaGraphExec_t exec[2] = {nullptr, nullptr};
     cudaStream_t cap = nullptr;
@@ -781,13 +805,13 @@ int64_t gbEulerRun(cuMesh* mesh, FvmField* rho, FvmField* rhou, FvmField* rhoe, 
         cudaGraph_t g = nullptr;
         ok = cuda_ok(cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal), "graph capture");
         if (!ok) break;
-        for (int b = 0; b < n_bc; ++b) {
+        for (int b = 0; b < n_bc && !inline_bcs; ++b) {
             if (bcs[b].type == 0) enqueue_slip(mesh, rho, rhou, rhoe, (int)bcs[b].region_id, k, cap);
             else enqueue_farfield(mesh, rho, rhou, rhoe, (int)bcs[b].region_id, k, bcs[b].mach, bcs[b].pressure,
                                   bcs[b].temperature, cap);
         }
         launch_grad_lim(mi->dev, state_of(rho, rhou, rhoe, k), grad_of(rho, rhou, rhoe, false),
-                        g_transposed.load() != 0, cap);
+                        g_transposed.load() != 0, cap, inline_bcs ? &gbt : nullptr);
         enqueue_flux(mesh, rho, rhou, rhoe, error, cfl, k, cap);
         launch_reduce_final(nb, ei->partials, out, d_hist, d_counter, cap);
         ok = cuda_ok(cudaStreamEndCapture(cap, &g), "graph capture") &&
@@ -795,7 +819,7 @@ int64_t gbEulerRun(cuMesh* mesh, FvmField* rho, FvmField* rhou, FvmField* rhoe, 
         if (g) cudaGraphDestroy(g);
     }
     t_counting = true;
-    const int per_iter = n_bc + 3;
+    const int per_iter = (inline_bcs ? 0 : n_bc) + 3;
     int cur = impl(rho)->cur;
     int64_t done = 0;
     std::vector<double> hist((size_t)n_iter, 0.0);

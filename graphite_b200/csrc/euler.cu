@@ -101,9 +101,9 @@ __global__ void __launch_bounds__(kBlock, kGradBlocksPerSM) k_grad_lim(MeshDev m
 #endif
 constexpr int kStageThreads = GB_GRAD_STAGE_THREADS;
 
-template <bool TRANSPOSED>
+template <bool TRANSPOSED, typename Ghosts>
 __global__ void __launch_bounds__(kStageThreads, GB_GRAD_STAGE_BLOCKS)
-    k_grad_lim_staged(MeshDev m, EulerState q, EulerGrad g) {
+    k_grad_lim_staged(MeshDev m, EulerState q, EulerGrad g, Ghosts gh) {
     constexpr int B = kStageThreads;
     __shared__ float4 s_dn[kSlots * B], s_df[kSlots * B];
     __shared__ uint32_t s_nbc[kSlots * B], s_twin[kSlots * B];
@@ -119,7 +119,8 @@ __global__ void __launch_bounds__(kStageThreads, GB_GRAD_STAGE_BLOCKS)
         cp_async4(&s_twin[t * B + tid], &m.twin[k]);
     }
     asm volatile("cp.async.commit_group;\n" ::: "memory");
-    grad_lim_cell<TRANSPOSED>(m, q, g, i, nf, EntriesStaged<B>{s_nbc + tid, s_dn + tid, s_df + tid, s_twin + tid});
+    grad_lim_cell<TRANSPOSED>(m, q, g, i, nf, EntriesStaged<B>{s_nbc + tid, s_dn + tid, s_df + tid, s_twin + tid},
+                              gh);
 }
 
 // Fused flux / local-time-step update / squared residual over the interior
@@ -227,12 +228,19 @@ void launch_entry_geo(const DevMesh& m, cudaStream_t s) {
     count_launch();
 }
 
-void launch_grad_lim(const DevMesh& m, EulerState q, EulerGrad g, bool transposed, cudaStream_t s) {
+void launch_grad_lim(const DevMesh& m, EulerState q, EulerGrad g, bool transposed, cudaStream_t s,
+                     const GhostBcTable* ghosts) {
     if (m.N == 0) return;
 #if GB_GRAD_STAGED
     const unsigned gs = (unsigned)((m.N + kStageThreads - 1) / kStageThreads);
-    if (transposed) k_grad_lim_staged<true><<<gs, kStageThreads, 0, s>>>(mesh_dev(m), q, g);
-    else k_grad_lim_staged<false><<<gs, kStageThreads, 0, s>>>(mesh_dev(m), q, g);
+    const MeshDev md = mesh_dev(m);
+    if (ghosts) {
+        if (transposed) k_grad_lim_staged<true><<<gs, kStageThreads, 0, s>>>(md, q, g, GhostBcs{*ghosts});
+        else k_grad_lim_staged<false><<<gs, kStageThreads, 0, s>>>(md, q, g, GhostBcs{*ghosts});
+    } else {
+        if (transposed) k_grad_lim_staged<true><<<gs, kStageThreads, 0, s>>>(md, q, g, NoGhostBcs{});
+        else k_grad_lim_staged<false><<<gs, kStageThreads, 0, s>>>(md, q, g, NoGhostBcs{});
+    }
 #else
     if (transposed) k_grad_lim<true><<<grid(m.N), kBlock, 0, s>>>(mesh_dev(m), q, g);
     else k_grad_lim<false><<<grid(m.N), kBlock, 0, s>>>(mesh_dev(m), q, g);

@@ -194,6 +194,30 @@ struct NoGhostBcs {
     __device__ __forceinline__ void store(uint32_t, float, float4, float) const {}
 };
 
+// GhostBcTable (gb_device.cuh) as a Ghosts policy.
+struct GhostBcs {
+    static constexpr bool kActive = true;
+    GhostBcTable t;
+    // j: the ghost's cell index
+    __device__ __forceinline__ bool state(uint32_t j, float3 nrm, float r1, float3 u1, float e1, float& r, float4& ru,
+                                          float& e) const {
+        int k = 0;
+        while (k < t.n - 1 && j >= t.start[k + 1]) ++k;
+        if (t.type[k] < 0) return false;
+        if (t.type[k] == 0) slip_state(nrm, r1, u1, e1, r, ru, e);
+        else farfield_state(nrm, r1, u1, e1, t.mach[k], t.p[k], t.temp[k], r, ru, e);
+        return true;
+    }
+    __device__ __forceinline__ void store(uint32_t j, float r, float4 ru, float e) const {
+#pragma unroll
+        for (int b = 0; b < 2; ++b) {
+            t.rho[b][j] = r;
+            t.rhou[b][j] = ru;
+            t.rhoe[b][j] = e;
+        }
+    }
+};
+
 // Per-face entry data of cell i (slot t = 0..nf-1), read straight from the
 // slot-major arrays at entry i + t N.
 struct EntriesGlobal {

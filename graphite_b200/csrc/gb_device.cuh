@@ -103,7 +103,24 @@ void launch_bc_slip(const DevMesh& m, uint32_t g0, uint32_t g1, float* rho[2], f
 void launch_bc_farfield(const DevMesh& m, uint32_t g0, uint32_t g1, float* rho[2], float4* rhou[2],
                         float* rhoe[2], int cur, float3 mach, float p, float t, cudaStream_t s);
 void launch_entry_geo(const DevMesh& m, cudaStream_t s);
-void launch_grad_lim(const DevMesh& m, EulerState q, EulerGrad g, bool transposed, cudaStream_t s);
+// Boundary conditions the Euler gradient pass applies itself, by ghost
+// region: ghosts [start[r], start[r+1]) (absolute cell indices) get type[r]:
+// -1 none (their stored state), 0 slip, 1 far field with mach[r], p[r],
+// temp[r]; the computed ghost states are stored into both value buffers.
+constexpr int kMaxBcRegions = 16;
+struct GhostBcTable {
+    int n;
+    uint32_t start[kMaxBcRegions + 1];
+    int type[kMaxBcRegions];
+    float3 mach[kMaxBcRegions];
+    float p[kMaxBcRegions], temp[kMaxBcRegions];
+    float* rho[2];
+    float4* rhou[2];
+    float* rhoe[2];
+};
+
+void launch_grad_lim(const DevMesh& m, EulerState q, EulerGrad g, bool transposed, cudaStream_t s,
+                     const GhostBcTable* ghosts = nullptr);
 
 // Boundary conditions of the incompressible path applied by its gradient
 // kernel, by ghost region: ghosts [start[r], start[r+1]) (absolute cell
