@@ -28,9 +28,16 @@ __device__ __forceinline__ float3 operator-(float3 a, float3 b) { return make_fl
 __device__ __forceinline__ float3 operator*(float3 a, float b) { return make_float3(a.x * b, a.y * b, a.z * b); }
 __device__ __forceinline__ float dot(float3 a, float3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
 __device__ __forceinline__ float norm(float3 a) { return sqrtf(dot(a, a)); }
+// Explicitly rounded dot product (its multiply-adds fused in a fixed order):
+// the boundary states below are formed by several kernels (the ghost kernels
+// and the gradient kernels that apply the conditions themselves) and must come
+// out bitwise the same in each, whatever the compiler would fuse in context.
+__device__ __forceinline__ float xdot(float3 a, float3 b) {
+    return __fmaf_rn(a.z, b.z, __fmaf_rn(a.y, b.y, __fmul_rn(a.x, b.x)));
+}
 // include/datatypes.cuh:144-150: n * sign(n . d) with sign(0) = +1
 __device__ __forceinline__ float3 outer_normal(float3 n, float3 d) {
-    return dot(n, d) >= 0.f ? n : make_float3(-n.x, -n.y, -n.z);
+    return xdot(n, d) >= 0.f ? n : make_float3(-n.x, -n.y, -n.z);
 }
 // include/datatypes.cuh:375-377
 __device__ __forceinline__ float lsqrt(float x) { return sqrtf(fmaxf(1e-12f, fminf(1e30f, x))); }
@@ -114,8 +121,8 @@ __device__ __forceinline__ void reconstruct(float r, float4 u, float e, float4 g
 __device__ __forceinline__ void slip_state(float3 n, float r1, float3 u, float e1, float& r, float4& ru, float& e) {
     r = r1;
     e = e1;
-    const float3 ug = u - n * (2.f * dot(n, u));
-    ru = make_float4(ug.x, ug.y, ug.z, 0.f);
+    const float s = __fmul_rn(2.f, xdot(n, u));
+    ru = make_float4(__fmaf_rn(-n.x, s, u.x), __fmaf_rn(-n.y, s, u.y), __fmaf_rn(-n.z, s, u.z), 0.f);
 }
 
 // The outward normal of boundary face gl = (interior cell, face); the same
@@ -139,33 +146,35 @@ __device__ __forceinline__ void slip_ghost(const float4* __restrict__ cell_geo, 
 // (r1, ru1, e1) is the interior state, n the outward normal.
 __device__ __forceinline__ void farfield_state(float3 n, float r1, float3 ru1, float e1, float3 imach, float ip,
                                                float it, float& r, float4& ru4, float& e) {
-    const float3 u = ru1 * (1.f / r1);
-    const float p = 0.4f * (e1 - 0.5f / r1 * dot(ru1, ru1));
+    // every multiply-add explicitly rounded (see xdot)
+    auto scale = [](float3 a, float k) { return make_float3(__fmul_rn(a.x, k), __fmul_rn(a.y, k), __fmul_rn(a.z, k)); };
+    const float3 u = scale(ru1, 1.f / r1);
+    const float p = __fmul_rn(0.4f, __fmaf_rn(-(0.5f / r1), xdot(ru1, ru1), e1));
     const float tt = p / r1;
-    const float mach = sqrtf(dot(u, u) / (1.4f * p / r1));
+    const float mach = sqrtf(xdot(u, u) / (__fmul_rn(1.4f, p) / r1));
     const float idens = ip / it;
     float3 ru;
-    if (dot(u, n) < 0.f) {
+    if (xdot(u, n) < 0.f) {
         if (mach > 1.f) {
-            const float ic = sqrtf(1.4f * ip / idens);
-            const float3 iv = imach * ic;
+            const float ic = sqrtf(__fmul_rn(1.4f, ip) / idens);
+            const float3 iv = scale(imach, ic);
             r = idens;
-            ru = imach * ic * idens;
-            e = ip / 0.4f + 0.5f * idens * dot(iv, iv);
+            ru = scale(iv, idens);
+            e = __fmaf_rn(__fmul_rn(0.5f, idens), xdot(iv, iv), ip / 0.4f);
         } else {
             r = p / it;
-            const float ic = sqrtf(1.4f * p / r);
-            const float3 v = imach * ic;
-            ru = v * r;
-            e = p / 0.4f + 0.5f * r * dot(v, v);
+            const float ic = sqrtf(__fmul_rn(1.4f, p) / r);
+            const float3 v = scale(imach, ic);
+            ru = scale(v, r);
+            e = __fmaf_rn(__fmul_rn(0.5f, r), xdot(v, v), p / 0.4f);
         }
     } else {
         if (mach > 1.f) {
             r = r1; ru = ru1; e = e1;
         } else {
             r = ip / tt;
-            ru = u * r;
-            e = ip / 0.4f + 0.5f * r * dot(u, u);
+            ru = scale(u, r);
+            e = __fmaf_rn(__fmul_rn(0.5f, r), xdot(u, u), ip / 0.4f);
         }
     }
     ru4 = make_float4(ru.x, ru.y, ru.z, 0.f);

@@ -43,13 +43,16 @@ __global__ void k_nsi_init(int64_t n, float* p, float4* u, float p0, float3 u0) 
 // outward normal n.
 __device__ __forceinline__ void nsi_ghost_state(int type, float3 n, float pi, float3 ui, float3 vinf, float pinf,
                                                 float& pg, float3& ug) {
+    // explicitly rounded (xdot): the ghost kernel and the gradient kernel both
+    // form these states and must agree bitwise
     if (type == 0) {
-        ug = ui - n * (2.f * dot(n, ui));
+        const float s = __fmul_rn(2.f, xdot(n, ui));
+        ug = make_float3(__fmaf_rn(-n.x, s, ui.x), __fmaf_rn(-n.y, s, ui.y), __fmaf_rn(-n.z, s, ui.z));
         pg = pi;
     } else if (type == 2) {
         ug = make_float3(-ui.x, -ui.y, -ui.z);
         pg = pi;
-    } else if (dot(vinf, n) < 0.f) {
+    } else if (xdot(vinf, n) < 0.f) {
         ug = vinf;
         pg = pi;
     } else {
