@@ -772,14 +772,17 @@ int64_t gbEulerRun(cuMesh* mesh, FvmField* rho, FvmField* rhou, FvmField* rhoe, 
         return -1;
     }
     double* out = mi->dev.red + mi->dev.n_red_max;
-    // On ghost-heavy meshes (one-layer extrusions carry two span ghosts per
-    // cell) the gradient kernel applies the boundary conditions itself
-    // (GhostBcTable); on the others the ghost kernels cost less than the
-    // extra work in the gradient pass.
+    // The boundary conditions as a table by ghost region.  On ghost-heavy
+    // meshes (one-layer extrusions carry two span ghosts per cell) the
+    // gradient kernel applies them itself; on the others one ghost kernel
+    // applies all regions' conditions (it costs less than the extra work in
+    // the gradient pass).  Meshes with more regions than the table holds use
+    // one ghost kernel per condition.
     const int n_regions = (int)mi->topo.regions.size();
-    const bool inline_bcs = n_regions > 0 && n_regions <= kMaxBcRegions && 4 * mi->dev.G >= mi->dev.N;
+    const bool table_bcs = n_regions > 0 && n_regions <= kMaxBcRegions;
+    const bool inline_bcs = table_bcs && 4 * mi->dev.G >= mi->dev.N;
     GhostBcTable gbt{};
-    if (inline_bcs) {
+    if (table_bcs) {
         gbt.n = n_regions;
         for (int r = 0; r <= n_regions; ++r) gbt.start[r] = mi->num.region_start[r];
         for (int r = 0; r < n_regions; ++r) gbt.type[r] = -1;
@@ -805,7 +808,8 @@ int64_t gbEulerRun(cuMesh* mesh, FvmField* rho, FvmField* rhou, FvmField* rhoe, 
         cudaGraph_t g = nullptr;
         ok = cuda_ok(cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal), "graph capture");
         if (!ok) break;
-        for (int b = 0; b < n_bc && !inline_bcs; ++b) {
+        if (table_bcs && !inline_bcs && n_bc > 0) launch_bc_table(mi->dev, gbt, k, cap);
+        for (int b = 0; b < n_bc && !table_bcs; ++b) {
             if (bcs[b].type == 0) enqueue_slip(mesh, rho, rhou, rhoe, (int)bcs[b].region_id, k, cap);
             else enqueue_farfield(mesh, rho, rhou, rhoe, (int)bcs[b].region_id, k, bcs[b].mach, bcs[b].pressure,
                                   bcs[b].temperature, cap);
@@ -819,7 +823,7 @@ int64_t gbEulerRun(cuMesh* mesh, FvmField* rho, FvmField* rhou, FvmField* rhoe, 
         if (g) cudaGraphDestroy(g);
     }
     t_counting = true;
-    const int per_iter = (inline_bcs ? 0 : n_bc) + 3;
+    const int per_iter = (inline_bcs ? 0 : (table_bcs ? (n_bc > 0 ? 1 : 0) : n_bc)) + 3;
     int cur = impl(rho)->cur;
     int64_t done = 0;
     std::vector<double> hist((size_t)n_iter, 0.0);

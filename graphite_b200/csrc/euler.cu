@@ -81,6 +81,31 @@ __global__ void k_bc_farfield(uint32_t g0, uint32_t g1, uint32_t N, const float4
     }
 }
 
+// All regions' boundary conditions in one launch, from a GhostBcTable: ghost
+// t takes its region's condition (the same slip_ghost / farfield_ghost as the
+// per-region kernels; regions of type -1 are left as they are).
+__global__ void k_bc_table(uint32_t N, uint32_t G, const float4* __restrict__ cell_geo,
+                           const float4* __restrict__ face_geo, const uint2* __restrict__ ghost, GhostBcTable tb,
+                           int cur) {
+    const uint32_t t = N + blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= N + G) return;
+    int k = 0;
+    while (k < tb.n - 1 && t >= tb.start[k + 1]) ++k;
+    if (tb.type[k] < 0) return;
+    float r, e;
+    float4 ru;
+    if (tb.type[k] == 0)
+        slip_ghost(cell_geo, face_geo, ghost[t - N], tb.rho[cur], tb.rhou[cur], tb.rhoe[cur], r, ru, e);
+    else
+        farfield_ghost(cell_geo, face_geo, ghost[t - N], tb.rho[cur], tb.rhou[cur], tb.rhoe[cur], tb.mach[k], tb.p[k],
+                       tb.temp[k], r, ru, e);
+    for (int b = 0; b < 2; ++b) {
+        tb.rho[b][t] = r;
+        tb.rhou[b][t] = ru;
+        tb.rhoe[b][t] = e;
+    }
+}
+
 // Fused FvmEulerStepPrepare over the interior cells of one mesh: gradients,
 // limiters and the reconstructed face states.
 template <bool TRANSPOSED>
@@ -214,6 +239,12 @@ void launch_bc_farfield(const DevMesh& m, uint32_t g0, uint32_t g1, float* rho[2
     GhostBuf b = {{rho[0], rho[1]}, {rhou[0], rhou[1]}, {rhoe[0], rhoe[1]}};
     k_bc_farfield<<<grid(g1 - g0), kBlock, 0, s>>>(g0, g1, (uint32_t)m.N, m.cell_geo, m.face_geo, m.ghost, b, cur,
                                                    mach, p, t);
+    count_launch();
+}
+
+void launch_bc_table(const DevMesh& m, const GhostBcTable& t, int cur, cudaStream_t s) {
+    if (m.G == 0) return;
+    k_bc_table<<<grid(m.G), kBlock, 0, s>>>((uint32_t)m.N, (uint32_t)m.G, m.cell_geo, m.face_geo, m.ghost, t, cur);
     count_launch();
 }
 

@@ -121,6 +121,8 @@ struct GhostBcTable {
 
 void launch_grad_lim(const DevMesh& m, EulerState q, EulerGrad g, bool transposed, cudaStream_t s,
                      const GhostBcTable* ghosts = nullptr);
+// every region's condition of the table in one ghost kernel (reads buffer cur)
+void launch_bc_table(const DevMesh& m, const GhostBcTable& t, int cur, cudaStream_t s);
 
 // Boundary conditions of the incompressible path applied by its gradient
 // kernel, by ghost region: ghosts [start[r], start[r+1]) (absolute cell
