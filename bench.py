@@ -202,7 +202,7 @@ def byte_model(case):
     rec = 4 + 16                # reconstructed rho, (rho u, rho E)
     grad_lim = {
         "ghost_cell_geo": 16 * G, "state": state * NG, "faces_per_cell": N, "lsq": 32 * N,
-        "entry_nbr_weight_face": (4 + 16 + 16 + 4) * S, "ghost_entries": (8 + 16) * G,
+        "entry_nbr_weight_face": (4 + 16 + 16) * S, "ghost_entries": (8 + 16) * G,
         "face_state_write": rec * (S + G), "grad_write": 80 * N}
     flux = {
         "cell_volume": 16 * N, "faces_per_cell": N, "entry_twin_normal": (4 + 16) * S, "face_states": rec * (S + G),

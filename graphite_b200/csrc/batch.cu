@@ -137,7 +137,7 @@ __global__ void __launch_bounds__(kStagedThreads, kStagedBlocks)
                         int tile, const BcDev* __restrict__ bcs) {
     constexpr int B = kStagedThreads;
     __shared__ float4 s_dn[kSlots * B], s_df[kSlots * B];
-    __shared__ uint32_t s_nbc[kSlots * B], s_twin[kSlots * B];
+    __shared__ uint32_t s_nbc[kSlots * B];
     const int2 w = items[blockIdx.x];
     const InstDev& I = insts[w.x];
     if (I.status) return;
@@ -159,10 +159,9 @@ __global__ void __launch_bounds__(kStagedThreads, kStagedBlocks)
             cp_async4(&s_nbc[t * B + tid], &m.nbc[k]);
             cp_async16(&s_dn[t * B + tid], &m.dn[k]);
             cp_async16(&s_df[t * B + tid], &m.df[k]);
-            cp_async4(&s_twin[t * B + tid], &m.twin[k]);
-        }
+            }
         asm volatile("cp.async.commit_group;\n" ::: "memory");
-        grad_lim_cell<TRANSPOSED>(m, q, g, i, nf, EntriesStaged<B>{s_nbc + tid, s_dn + tid, s_df + tid, s_twin + tid},
+        grad_lim_cell<TRANSPOSED>(m, q, g, i, nf, EntriesStaged<B>{s_nbc + tid, s_dn + tid, s_df + tid},
                                   gh);
     }
 }

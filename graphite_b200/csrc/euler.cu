@@ -115,14 +115,14 @@ __global__ void __launch_bounds__(kBlock, kGradBlocksPerSM) k_grad_lim(MeshDev m
 }
 
 // k_grad_lim with each cell's per-face entries (neighbour, LSQ offset, face
-// offset, twin) staged in shared memory by cp.async as the first thing the
+// offset: 36 B per face) staged in shared memory by cp.async as the first thing the
 // thread does: all of a cell's entry streams are in flight together while the
 // cell's own state loads, instead of one face per memory round trip.
 #ifndef GB_GRAD_STAGE_THREADS
 #define GB_GRAD_STAGE_THREADS 64
 #endif
 #ifndef GB_GRAD_STAGE_BLOCKS
-#define GB_GRAD_STAGE_BLOCKS 14
+#define GB_GRAD_STAGE_BLOCKS 15
 #endif
 constexpr int kStageThreads = GB_GRAD_STAGE_THREADS;
 
@@ -131,7 +131,7 @@ __global__ void __launch_bounds__(kStageThreads, GB_GRAD_STAGE_BLOCKS)
     k_grad_lim_staged(MeshDev m, EulerState q, EulerGrad g, Ghosts gh) {
     constexpr int B = kStageThreads;
     __shared__ float4 s_dn[kSlots * B], s_df[kSlots * B];
-    __shared__ uint32_t s_nbc[kSlots * B], s_twin[kSlots * B];
+    __shared__ uint32_t s_nbc[kSlots * B];
     const uint32_t tid = threadIdx.x;
     const uint32_t i = blockIdx.x * B + tid;
     if (i >= m.N) return;
@@ -141,10 +141,9 @@ __global__ void __launch_bounds__(kStageThreads, GB_GRAD_STAGE_BLOCKS)
         cp_async4(&s_nbc[t * B + tid], &m.nbc[k]);
         cp_async16(&s_dn[t * B + tid], &m.dn[k]);
         cp_async16(&s_df[t * B + tid], &m.df[k]);
-        cp_async4(&s_twin[t * B + tid], &m.twin[k]);
     }
     asm volatile("cp.async.commit_group;\n" ::: "memory");
-    grad_lim_cell<TRANSPOSED>(m, q, g, i, nf, EntriesStaged<B>{s_nbc + tid, s_dn + tid, s_df + tid, s_twin + tid},
+    grad_lim_cell<TRANSPOSED>(m, q, g, i, nf, EntriesStaged<B>{s_nbc + tid, s_dn + tid, s_df + tid},
                               gh);
 }
 

@@ -235,7 +235,6 @@ struct EntriesGlobal {
     __device__ __forceinline__ uint32_t nbc(uint32_t t) const { return __ldg(&m.nbc[i + t * m.N]); }
     __device__ __forceinline__ float4 dn(uint32_t t) const { return __ldg(&m.dn[i + t * m.N]); }
     __device__ __forceinline__ float4 df(uint32_t t) const { return __ldg(&m.df[i + t * m.N]); }
-    __device__ __forceinline__ uint32_t twin(uint32_t t) const { return __ldg(&m.twin[i + t * m.N]); }
     __device__ __forceinline__ void ready() const {}
 };
 
@@ -247,11 +246,9 @@ struct EntriesStaged {
     const uint32_t* s_nbc;
     const float4* s_dn;
     const float4* s_df;
-    const uint32_t* s_twin;
     __device__ __forceinline__ uint32_t nbc(uint32_t t) const { return s_nbc[t * B]; }
     __device__ __forceinline__ float4 dn(uint32_t t) const { return s_dn[t * B]; }
     __device__ __forceinline__ float4 df(uint32_t t) const { return s_df[t * B]; }
-    __device__ __forceinline__ uint32_t twin(uint32_t t) const { return s_twin[t * B]; }
     __device__ __forceinline__ void ready() const { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
 };
 
@@ -334,10 +331,11 @@ __device__ __forceinline__ void grad_lim_cell(const MeshDev& m, EulerState q, Eu
         reconstruct<TRANSPOSED>(v[0], u0, v[4], gr, gu, ge, f3(e.df(t)), rr, ru, re);
         g.rec_rho[k] = rr;
         g.rec_rhou[k] = make_float4(ru.x, ru.y, ru.z, re);
-        const uint32_t tw = e.twin(t);
-        if (tw >= m.S) {
-            // ghost neighbour: its state with this cell's gradient and limiter
-            const uint32_t j = m.N + (tw - m.S);
+        const uint32_t j = e.nbc(t);
+        if (j >= m.N) {
+            // ghost neighbour N + g: its state with this cell's gradient and
+            // limiter, stored at the ghost's face-state slot S + g
+            const uint32_t tw = m.S + (j - m.N);
             const float3 fc = f3(__ldg(&m.face_geo[2 * __ldg(&m.nb[k]).x + 1]));
             float rj, ej;
             float4 uj;
