@@ -53,14 +53,18 @@ def test_converter_matches_reference_converter(name, su2_paths, workdir):
     assert rr == mr
 
 
-def test_parallel_converter_matches_oracle_topology(workdir):
-    """At 216k elements the converter builds the face records, sorts them and
-    numbers the faces on several host threads; its file equals the oracle's
-    serial topology (both number faces in first-appearance order) exactly."""
+@pytest.mark.parametrize("cells,shape", [("tet", (60, 30, 20)), ("hex", (60, 40, 60)), ("prism", (60, 30, 40)),
+                                         ("pyramid", (60, 30, 13))])
+def test_parallel_converter_matches_oracle_topology(workdir, cells, shape):
+    """With 130k-216k elements the converter builds the face records, sorts
+    them and numbers the faces on several host threads; its file equals the
+    oracle's serial topology (both number faces in first-appearance order)
+    exactly, for triangle faces, quad faces and both mixed."""
     from graphite_b200 import meshgen
     from oracle import OracleMesh
-    mesh = meshgen.channel_bump(nx=60, ny=30, nz=20, cells="tet")
-    su2, out = str(workdir / "par.su2"), str(workdir / "par.fvm")
+    nx, ny, nz = shape
+    mesh = meshgen.channel_bump(nx=nx, ny=ny, nz=nz, cells=cells)
+    su2, out = str(workdir / f"par_{cells}.su2"), str(workdir / f"par_{cells}.fvm")
     mesh.write_su2(su2)
     assert capi.load().cuMeshFromSu2(su2.encode(), out.encode()) == 0, capi.last_error()
     nodes, faces, cells, regions = read_fvm(out)
