@@ -242,7 +242,14 @@ typedef struct gbBc {
  * array of n_iter doubles, may be NULL).  Stops early, after the iteration
  * in which residual/residual[0] < tolerance, when tolerance > 0 (checked
  * every check_every iterations; the residuals between checks are still
- * recorded).  Returns the number of iterations run, or -1 on error. */
+ * recorded).  Returns the number of iterations run, or -1 on error.
+ * The results, ghost values included, are bitwise those of the per-call
+ * loop (FvmEuler*Bc, FvmEulerStepPrepare, FvmEulerStep, FvmFieldReduceSum);
+ * where a region appears twice in bcs the later condition holds, and the
+ * gradients and limiters of the fields are not stored (the per-call
+ * FvmEulerStepPrepare stores them).  Inside, all conditions are applied by
+ * one ghost kernel, or, when the ghosts number at least a quarter of the
+ * cells, by the gradient kernel itself. */
 int64_t gbEulerRun(cuMesh* mesh, FvmField* rho, FvmField* rhou, FvmField* rhoe, FvmField* error,
                    gb_scalar cfl, int64_t n_iter, const gbBc* bcs, int n_bc, double tolerance,
                    int check_every, double* residual_history);
@@ -443,7 +450,9 @@ int FvmNSIStep(cuMesh* mesh, FvmField* velocity, FvmField* pressure, gb_scalar c
                FvmField* dt, FvmField* error);
 /* The whole loop as replayed graphs (as gbEulerRun).  Boundary conditions:
  * type 0 slip, 1 inlet / outlet (mach = inlet velocity, pressure = outlet
- * pressure), 2 no-slip wall. */
+ * pressure), 2 no-slip wall.  The results, ghost values included, are
+ * bitwise those of the per-call loop; when the ghosts number at least a
+ * quarter of the cells the gradient kernel applies the conditions itself. */
 int64_t gbNSIRun(cuMesh* mesh, FvmField* velocity, FvmField* pressure, FvmField* error, gb_scalar cfl,
                  int64_t n_iter, const gbBc* bcs, int n_bc, double tolerance, int check_every,
                  double* residual_history);
