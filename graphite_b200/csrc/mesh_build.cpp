@@ -235,17 +235,17 @@ inline bool rec_less(const FaceRec& x, const FaceRec& y) {
     return x.lf < y.lf;
 }
 
-// Sorts the records on the host's hardware threads: chunks sorted in
-// parallel, then merged pairwise, in parallel, log2(chunks) rounds.  The
-// order is total (no two records are equal), so the result is the same as a
-// serial sort's.
-void parallel_sort(std::vector<FaceRec>& v) {
+// Sorts v by less on the host's hardware threads: chunks sorted in parallel,
+// then merged pairwise, in parallel, log2(chunks) rounds.  With a total order
+// (no two records equal) the result is the same as a serial sort's.
+template <typename T, typename Less>
+void parallel_sort_by(std::vector<T>& v, Less less) {
     const size_t n = v.size();
     unsigned hw = std::thread::hardware_concurrency();
     size_t chunks = 1;
     while (chunks * 2 <= std::min<size_t>(hw ? hw : 1, 32) && n / (chunks * 2) >= 65536) chunks *= 2;
     if (chunks == 1) {
-        std::sort(v.begin(), v.end(), rec_less);
+        std::sort(v.begin(), v.end(), less);
         return;
     }
     std::vector<size_t> cut(chunks + 1);
@@ -253,7 +253,7 @@ void parallel_sort(std::vector<FaceRec>& v) {
     {
         std::vector<std::thread> th;
         for (size_t c = 0; c < chunks; ++c)
-            th.emplace_back([&, c] { std::sort(v.begin() + cut[c], v.begin() + cut[c + 1], rec_less); });
+            th.emplace_back([&, c] { std::sort(v.begin() + cut[c], v.begin() + cut[c + 1], less); });
         for (auto& t : th) t.join();
     }
     for (size_t w = 1; w < chunks; w *= 2) {
@@ -261,7 +261,7 @@ void parallel_sort(std::vector<FaceRec>& v) {
         for (size_t c = 0; c + w < chunks; c += 2 * w) {
             const size_t lo = cut[c], mid = cut[c + w], hi = cut[std::min(c + 2 * w, chunks)];
             th.emplace_back([&, lo, mid, hi] {
-                std::inplace_merge(v.begin() + lo, v.begin() + mid, v.begin() + hi, rec_less);
+                std::inplace_merge(v.begin() + lo, v.begin() + mid, v.begin() + hi, less);
             });
         }
         for (auto& t : th) t.join();
@@ -313,7 +313,7 @@ bool build_topology(const ElementSet& es, Topology& t) {
             }
         }
     });
-    parallel_sort(srt);
+    parallel_sort_by(srt, rec_less);
     auto rec_index = [&](const FaceRec& r) { return (uint32_t)(rec_off[r.cell] + r.lf); };
     // groups of equal keys
     std::vector<uint32_t> group_of(S);
@@ -635,9 +635,14 @@ void number_cells(const Topology& t, bool rcm, Numbering& num) {
                     uint32_t v = t.cc[k];
                     if (v < (uint32_t)N && !done[v]) { done[v] = 1; nbrs.push_back(v); }
                 }
-                std::sort(nbrs.begin(), nbrs.end(), [&](uint32_t a, uint32_t b) {
-                    return deg[a] != deg[b] ? deg[a] < deg[b] : a < b;
-                });
+                // at most a handful: insertion sort by (degree, index)
+                for (size_t x = 1; x < nbrs.size(); ++x) {
+                    const uint32_t v = nbrs[x];
+                    size_t y = x;
+                    for (; y > 0 && (deg[nbrs[y - 1]] != deg[v] ? deg[nbrs[y - 1]] > deg[v] : nbrs[y - 1] > v); --y)
+                        nbrs[y] = nbrs[y - 1];
+                    nbrs[y] = v;
+                }
                 for (uint32_t v : nbrs) order.push_back(v);
             }
         }
@@ -672,11 +677,17 @@ void number_cells(const Topology& t, bool rcm, Numbering& num) {
             fa[f] = std::min(a, b);
             fb[f] = std::max(a, b);
         }
-    num.face_old.resize(F);
-    std::iota(num.face_old.begin(), num.face_old.end(), 0u);
-    std::sort(num.face_old.begin(), num.face_old.end(), [&](uint32_t x, uint32_t y) {
-        return fa[x] != fa[y] ? fa[x] < fa[y] : (fb[x] != fb[y] ? fb[x] < fb[y] : x < y);
+    // sort (lower, higher, face id) as one 64-bit key plus the id: direct
+    // comparisons on contiguous records, in parallel chunks
+    std::vector<std::pair<uint64_t, uint32_t>> keyed(F);
+    parallel_ranges(F, [&](int64_t f0, int64_t f1) {
+        for (int64_t f = f0; f < f1; ++f) keyed[f] = {((uint64_t)fa[f] << 32) | fb[f], (uint32_t)f};
     });
+    parallel_sort_by(keyed, [](const std::pair<uint64_t, uint32_t>& x, const std::pair<uint64_t, uint32_t>& y) {
+        return x.first != y.first ? x.first < y.first : x.second < y.second;
+    });
+    num.face_old.resize(F);
+    for (int64_t i = 0; i < F; ++i) num.face_old[i] = keyed[i].second;
     num.face_new.resize(F);
     for (int64_t i = 0; i < F; ++i) num.face_new[num.face_old[i]] = (uint32_t)i;
     // interior CSR in new order, element-local face order kept
