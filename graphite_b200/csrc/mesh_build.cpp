@@ -2,6 +2,7 @@
 // reference's cell/face/ghost topology, the .fvm file format, and the device
 // numbering (reverse Cuthill-McKee).
 #include <algorithm>
+#include <mutex>
 #include <thread>
 #include <cerrno>
 #include <cstdio>
@@ -88,6 +89,21 @@ struct Lines {
     }
 };
 
+// Runs fn(lo, hi) over [0, n) split into contiguous ranges, one per host
+// thread (at most 32).
+template <typename Fn>
+void parallel_ranges(int64_t n, Fn fn) {
+    const unsigned hw = std::thread::hardware_concurrency();
+    const int64_t parts = std::max<int64_t>(1, std::min<int64_t>({(int64_t)(hw ? hw : 1), 32, n / 65536}));
+    if (parts == 1) {
+        fn((int64_t)0, n);
+        return;
+    }
+    std::vector<std::thread> th;
+    for (int64_t p = 0; p < parts; ++p) th.emplace_back(fn, n * p / parts, n * (p + 1) / parts);
+    for (auto& t : th) t.join();
+}
+
 bool keyword(char* line, const char* kw, char** rest) {
     size_t n = strlen(kw);
     if (strncmp(line, kw, n) != 0) return false;
@@ -124,42 +140,79 @@ bool parse_su2(const char* path, ElementSet& es) {
         } else if (keyword(line, "NELEM=", &rest)) {
             int64_t n;
             if (!parse_count(rest, n)) return bad("bad NELEM");
-            es.kinds.reserve(n);
-            es.eoff.reserve(n + 1);
-            es.enodes.reserve(n * 6);
-            for (int64_t e = 0; e < n; ++e) {
-                char* l = L.next();
-                if (!l) return bad("unexpected end of file in NELEM block");
-                char* p = l;
-                long kind = strtol(p, &p, 10);
-                int k = nodes_of_kind((int)kind);
-                if (k == 0 || kind == 5 || kind == 9)
-                    return bad("element " + std::to_string(e) + ": unsupported volume element kind " + std::to_string(kind));
-                for (int j = 0; j < k; ++j) {
-                    char* q;
-                    unsigned long v = strtoul(p, &q, 10);
-                    if (q == p) return bad("element " + std::to_string(e) + ": too few nodes");
-                    p = q;
-                    es.enodes.push_back((uint32_t)v);
+            // line pointers in order, then each element's kind and nodes parsed
+            // on all host threads into a fixed-stride scratch array (at most 8
+            // nodes), then compacted; an error names the first bad element,
+            // with the check that fails first on its line (kind, then nodes)
+            std::vector<char*> lines((size_t)n);
+            for (int64_t e = 0; e < n; ++e)
+                if (!(lines[e] = L.next())) return bad("unexpected end of file in NELEM block");
+            es.kinds.resize(n);
+            std::vector<uint32_t> scratch((size_t)n * 8);
+            int64_t first_bad = n;
+            bool bad_kind = false;
+            std::mutex bad_mu;
+            parallel_ranges(n, [&](int64_t e0, int64_t e1) {
+                for (int64_t e = e0; e < e1; ++e) {
+                    char* p = lines[e];
+                    const long kind = strtol(p, &p, 10);
+                    const int k = nodes_of_kind((int)kind);
+                    bool kind_fails = k == 0 || kind == 5 || kind == 9, nodes_fail = false;
+                    for (int j = 0; j < k && !kind_fails; ++j) {
+                        char* q;
+                        const unsigned long v = strtoul(p, &q, 10);
+                        if (q == p) { nodes_fail = true; break; }
+                        p = q;
+                        scratch[8 * e + j] = (uint32_t)v;
+                    }
+                    if (kind_fails || nodes_fail) {   // the first failure of this range
+                        std::lock_guard<std::mutex> g(bad_mu);
+                        if (e < first_bad) { first_bad = e; bad_kind = kind_fails; }
+                        return;
+                    }
+                    es.kinds[e] = (int8_t)kind;
                 }
-                es.kinds.push_back((int8_t)kind);
-                es.eoff.push_back((int64_t)es.enodes.size());
+            });
+            if (first_bad < n) {
+                const int64_t e = first_bad;
+                if (bad_kind)
+                    return bad("element " + std::to_string(e) + ": unsupported volume element kind " +
+                               std::to_string(strtol(lines[e], nullptr, 10)));
+                return bad("element " + std::to_string(e) + ": too few nodes");
             }
+            es.eoff.resize(n + 1);
+            es.eoff[0] = 0;
+            for (int64_t e = 0; e < n; ++e) es.eoff[e + 1] = es.eoff[e] + nodes_of_kind(es.kinds[e]);
+            es.enodes.resize(es.eoff[n]);
+            parallel_ranges(n, [&](int64_t e0, int64_t e1) {
+                for (int64_t e = e0; e < e1; ++e)
+                    for (int64_t j = es.eoff[e]; j < es.eoff[e + 1]; ++j) es.enodes[j] = scratch[8 * e + (j - es.eoff[e])];
+            });
         } else if (keyword(line, "NPOIN=", &rest)) {
             if (!parse_count(rest, npoin)) return bad("bad NPOIN");
             es.nodes.resize(3 * npoin);
-            for (int64_t i = 0; i < npoin; ++i) {
-                char* l = L.next();
-                if (!l) return bad("unexpected end of file in NPOIN block");
-                char* p = l;
-                for (int c = 0; c < 3; ++c) {
-                    char* q;
-                    double v = strtod(p, &q);
-                    if (q == p) return bad("point " + std::to_string(i) + ": expected 3 coordinates");
-                    es.nodes[3 * i + c] = v;
-                    p = q;
+            std::vector<char*> lines((size_t)npoin);
+            for (int64_t i = 0; i < npoin; ++i)
+                if (!(lines[i] = L.next())) return bad("unexpected end of file in NPOIN block");
+            std::vector<int64_t> bad_at(1, npoin);
+            std::mutex bad_mu;
+            parallel_ranges(npoin, [&](int64_t i0, int64_t i1) {
+                for (int64_t i = i0; i < i1; ++i) {
+                    char* p = lines[i];
+                    for (int c = 0; c < 3; ++c) {
+                        char* q;
+                        const double v = strtod(p, &q);
+                        if (q == p) {
+                            std::lock_guard<std::mutex> g(bad_mu);
+                            bad_at[0] = std::min(bad_at[0], i);
+                            return;
+                        }
+                        es.nodes[3 * i + c] = v;
+                        p = q;
+                    }
                 }
-            }
+            });
+            if (bad_at[0] < npoin) return bad("point " + std::to_string(bad_at[0]) + ": expected 3 coordinates");
         } else if (keyword(line, "NMARK=", &rest)) {
             int64_t m;
             if (!parse_count(rest, m)) return bad("bad NMARK");
@@ -213,20 +266,6 @@ struct FaceRec {
     uint32_t lf;
 };
 
-// Runs fn(lo, hi) over [0, n) split into contiguous ranges, one per host
-// thread (at most 32).
-template <typename Fn>
-void parallel_ranges(int64_t n, Fn fn) {
-    const unsigned hw = std::thread::hardware_concurrency();
-    const int64_t parts = std::max<int64_t>(1, std::min<int64_t>({(int64_t)(hw ? hw : 1), 32, n / 65536}));
-    if (parts == 1) {
-        fn((int64_t)0, n);
-        return;
-    }
-    std::vector<std::thread> th;
-    for (int64_t p = 0; p < parts; ++p) th.emplace_back(fn, n * p / parts, n * (p + 1) / parts);
-    for (auto& t : th) t.join();
-}
 
 inline bool rec_less(const FaceRec& x, const FaceRec& y) {
     if (x.k0 != y.k0) return x.k0 < y.k0;

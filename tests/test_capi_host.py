@@ -80,6 +80,30 @@ def test_parallel_converter_matches_oracle_topology(workdir, cells, shape):
     assert [r[0] for r in regions] == list(mesh.markers)
 
 
+@pytest.mark.parametrize("first,second,message", [
+    ("few", "kind", "element 100: too few nodes"),
+    ("kind", "few", "element 100: unsupported volume element kind 7")])
+def test_parallel_parse_reports_the_first_bad_element(workdir, first, second, message):
+    """A 140k-element file parses on several host threads; with two bad
+    elements in different threads' ranges the error still names the first
+    one, with the check that fails first on its line."""
+    from graphite_b200 import meshgen
+    path = str(workdir / "two_errors.su2")
+    meshgen.channel_bump(nx=60, ny=30, nz=13, cells="tet").write_su2(path)
+    lines = open(path).read().split("\n")
+    start = next(i for i, l in enumerate(lines) if l.startswith("NELEM=")) + 1
+    def spoil(line, how):
+        parts = line.split()
+        return " ".join(parts[:3]) if how == "few" else " ".join(["7"] + parts[1:])
+    lines[start + 100] = spoil(lines[start + 100], first)
+    lines[start + 120000] = spoil(lines[start + 120000], second)
+    with open(path, "w") as f:
+        f.write("\n".join(lines))
+    out = str(workdir / "two_errors.fvm").encode()
+    assert capi.load().cuMeshFromSu2(path.encode(), out) != 0
+    assert message in capi.last_error(), capi.last_error()
+
+
 def _write(path, text):
     with open(path, "w") as f:
         f.write(text)
