@@ -496,61 +496,95 @@ bool build_topology(const ElementSet& es, Topology& t) {
 // .fvm layout, src/meshio.cu:1150-1216 (writer) and 166-292 (reader), float
 // node coordinates as in the reference's float build.
 bool write_fvm(const char* path, const Topology& t) {
-    FILE* f = fopen(path, "wb");
-    if (!f) { set_error(std::string("cannot write ") + path); return false; }
-    auto w32 = [&](uint32_t v) { fwrite(&v, 4, 1, f); };
+    // the whole file laid out in memory, then written at once
     const uint32_t nn = (uint32_t)(t.nodes.size() / 3);
+    const int64_t NG = t.N + t.G;
+    const size_t nr = t.regions.size();
+    const size_t bytes = 4 + 12 * (size_t)nn + 8 + 4 * ((size_t)t.F + t.fns[t.F]) + 8 + 4 * ((size_t)NG + 2 * (size_t)t.cfs[NG]) +
+                         8 + nr * (128 + 4) + 4 * (size_t)t.G;
+    std::vector<char> out(bytes);
+    char* w = out.data();
+    auto w32 = [&](uint32_t v) { memcpy(w, &v, 4); w += 4; };
+    auto warr = [&](const uint32_t* p, size_t n) { if (n) memcpy(w, p, 4 * n); w += 4 * n; };
     w32(nn);
-    std::vector<float> xyz(t.nodes.size());
-    for (size_t i = 0; i < t.nodes.size(); ++i) xyz[i] = (float)t.nodes[i];
-    fwrite(xyz.data(), 4, xyz.size(), f);
+    for (size_t i = 0; i < t.nodes.size(); ++i) {
+        const float x = (float)t.nodes[i];
+        memcpy(w, &x, 4);
+        w += 4;
+    }
     w32((uint32_t)t.F);
     w32(t.fns[t.F]);
     for (int64_t i = 0; i < t.F; ++i) {
         w32(t.fns[i + 1] - t.fns[i]);
-        fwrite(t.fn.data() + t.fns[i], 4, t.fns[i + 1] - t.fns[i], f);
+        warr(t.fn.data() + t.fns[i], t.fns[i + 1] - t.fns[i]);
     }
-    const int64_t NG = t.N + t.G;
     w32((uint32_t)NG);
     w32(t.cfs[NG]);
     for (int64_t i = 0; i < NG; ++i) {
         const uint32_t s = t.cfs[i], n = t.cfs[i + 1] - s;
         w32(n);
-        fwrite(t.cf.data() + s, 4, n, f);
-        fwrite(t.cc.data() + s, 4, n, f);
+        warr(t.cf.data() + s, n);
+        warr(t.cc.data() + s, n);
     }
-    const size_t nr = t.regions.size();
     w32((uint32_t)nr);
     w32((uint32_t)t.G);
     for (size_t r = 0; r < nr; ++r) {
         char name[128] = {0};
         strncpy(name, t.regions[r].c_str(), 127);
-        fwrite(name, 1, 128, f);
+        memcpy(w, name, 128);
+        w += 128;
         const uint32_t s = t.ghost_starts[r], e = t.ghost_starts[r + 1];
         w32(e - s);
-        fwrite(t.ghost_ids.data() + s, 4, e - s, f);
+        warr(t.ghost_ids.data() + s, e - s);
     }
-    const bool ok = ferror(f) == 0;
-    fclose(f);
+    FILE* f = fopen(path, "wb");
+    if (!f) { set_error(std::string("cannot write ") + path); return false; }
+    bool ok = (size_t)(w - out.data()) == bytes && fwrite(out.data(), 1, bytes, f) == bytes;
+    ok = (fclose(f) == 0) && ok;
     if (!ok) set_error(std::string("write error on ") + path);
     return ok;
 }
 
 bool read_fvm(const char* path, Topology& t) {
+    // the whole file read at once, then parsed from memory with every read
+    // checked against the bytes left
     FILE* f = fopen(path, "rb");
     if (!f) { set_error(std::string("cannot open mesh file ") + path); return false; }
+    std::vector<char> data;
+    {
+        fseek(f, 0, SEEK_END);
+        const long n = ftell(f);
+        fseek(f, 0, SEEK_SET);
+        data.resize(n > 0 ? (size_t)n : 0);
+        const size_t got = data.empty() ? 0 : fread(data.data(), 1, data.size(), f);
+        data.resize(got);
+        fclose(f);
+    }
     t = Topology();
-    bool ok = true;
-    auto r32 = [&](uint32_t& v) { if (fread(&v, 4, 1, f) != 1) ok = false; return ok; };
-    auto rarr = [&](uint32_t* p, size_t n) { if (n && fread(p, 4, n, f) != n) ok = false; return ok; };
-    auto fail = [&](const char* m) { fclose(f); set_error(std::string(path) + ": " + m); return false; };
+    size_t pos = 0;
+    auto left = [&]() { return data.size() - pos; };
+    auto r32 = [&](uint32_t& v) {
+        if (left() < 4) return false;
+        memcpy(&v, data.data() + pos, 4);
+        pos += 4;
+        return true;
+    };
+    auto rarr = [&](uint32_t* p, size_t n) {
+        if (left() / 4 < n) return false;
+        if (n) memcpy(p, data.data() + pos, 4 * n);
+        pos += 4 * n;
+        return true;
+    };
+    auto fail = [&](const char* m) { set_error(std::string(path) + ": " + m); return false; };
     uint32_t nn;
     if (!r32(nn)) return fail("truncated header");
+    if (left() / 12 < nn) return fail("truncated nodes");
     std::vector<float> xyz((size_t)nn * 3);
-    if (fread(xyz.data(), 4, xyz.size(), f) != xyz.size()) return fail("truncated nodes");
+    rarr(reinterpret_cast<uint32_t*>(xyz.data()), xyz.size());
     t.nodes.assign(xyz.begin(), xyz.end());
     uint32_t nf, nfn;
     if (!r32(nf) || !r32(nfn)) return fail("truncated faces header");
+    if (left() / 4 < (uint64_t)nf + nfn) return fail("truncated face nodes");
     t.F = nf;
     t.fns.resize((size_t)nf + 1);
     t.fn.resize(nfn);
@@ -565,6 +599,7 @@ bool read_fvm(const char* path, Topology& t) {
     t.fns[nf] = off;
     uint32_t ncg, ncf;
     if (!r32(ncg) || !r32(ncf)) return fail("truncated cells header");
+    if (left() / 4 < (uint64_t)ncg + 2 * (uint64_t)ncf) return fail("truncated cell record");
     t.cfs.resize((size_t)ncg + 1);
     t.cf.resize(ncf);
     t.cc.resize(ncf);
@@ -587,13 +622,15 @@ bool read_fvm(const char* path, Topology& t) {
     for (uint32_t r = 0; r < nr; ++r) {
         char name[129] = {0};
         uint32_t s;
-        if (fread(name, 1, 128, f) != 128 || !r32(s) || (uint64_t)off + s > ng) return fail("bad region record");
+        if (left() < 128) return fail("bad region record");
+        memcpy(name, data.data() + pos, 128);
+        pos += 128;
+        if (!r32(s) || (uint64_t)off + s > ng) return fail("bad region record");
         t.regions.emplace_back(name);
         if (!rarr(t.ghost_ids.data() + off, s)) return fail("truncated region");
         off += s;
         t.ghost_starts.push_back(off);
     }
-    fclose(f);
     if (off != ng) { set_error(std::string(path) + ": region sizes do not add up to the ghost count"); return false; }
     // validation the reference does not do
     for (uint32_t v : t.fn) if (v >= nn) { set_error(std::string(path) + ": face node out of range"); return false; }
