@@ -354,33 +354,54 @@ bool build_topology(const ElementSet& es, Topology& t) {
     });
     parallel_sort_by(srt, rec_less);
     auto rec_index = [&](const FaceRec& r) { return (uint32_t)(rec_off[r.cell] + r.lf); };
-    // groups of equal keys
-    std::vector<uint32_t> group_of(S);
-    std::vector<uint64_t> gk0, gk1;
-    std::vector<uint32_t> g_first;      // record index of the first (creating) element face
-    std::vector<uint32_t> g_cells;      // 2 per group
-    std::vector<uint8_t> g_count;
+    // groups of equal keys: a group starts where the key changes; group ids
+    // by a prefix sum over the starts; each group's arrays filled by its own
+    // records (the first writes the key, creator and count, the second the
+    // other cell), all in parallel.  A third record in a group is an error,
+    // reported for the first such record in key order.
+    std::vector<uint32_t> gid(S);
+    parallel_ranges(S, [&](int64_t i0, int64_t i1) {
+        for (int64_t i = i0; i < i1; ++i)
+            gid[i] = (i == 0 || srt[i].k0 != srt[i - 1].k0 || srt[i].k1 != srt[i - 1].k1) ? 1u : 0u;
+    });
+    int64_t n_groups = 0;
     for (int64_t i = 0; i < S; ++i) {
-        const FaceRec& r = srt[i];
-        const uint32_t ri = rec_index(r);
-        if (i == 0 || r.k0 != gk0.back() || r.k1 != gk1.back()) {
-            gk0.push_back(r.k0);
-            gk1.push_back(r.k1);
-            g_first.push_back(ri);
-            g_cells.push_back(r.cell);
-            g_cells.push_back(0xffffffffu);
-            g_count.push_back(1);
-        } else {
-            size_t g = gk0.size() - 1;
-            if (g_count[g] >= 2) {
-                set_error("non-manifold mesh: a face is shared by more than two elements (element " +
-                          std::to_string(r.cell) + ")");
-                return false;
+        const uint32_t start = gid[i];
+        n_groups += start;
+        gid[i] = (uint32_t)(n_groups - 1);
+    }
+    std::vector<uint32_t> group_of(S);
+    std::vector<uint64_t> gk0(n_groups), gk1(n_groups);
+    std::vector<uint32_t> g_first(n_groups);                  // record index of the first (creating) element face
+    std::vector<uint32_t> g_cells(2 * n_groups, 0xffffffffu); // 2 per group
+    std::vector<uint8_t> g_count(n_groups);
+    int64_t third = S;
+    std::mutex third_mu;
+    parallel_ranges(S, [&](int64_t i0, int64_t i1) {
+        for (int64_t i = i0; i < i1; ++i) {
+            const FaceRec& r = srt[i];
+            const uint32_t ri = rec_index(r);
+            const uint32_t g = gid[i];
+            group_of[ri] = g;
+            if (i == 0 || gid[i - 1] != g) {
+                gk0[g] = r.k0;
+                gk1[g] = r.k1;
+                g_first[g] = ri;
+                g_cells[2 * g] = r.cell;
+                g_count[g] = (i + 1 < S && gid[i + 1] == g) ? 2 : 1;
+            } else if (i < 2 || gid[i - 2] != g) {
+                g_cells[2 * g + 1] = r.cell;
+            } else {
+                std::lock_guard<std::mutex> lock(third_mu);
+                third = std::min(third, i);
+                return;
             }
-            g_cells[2 * g + 1] = r.cell;
-            g_count[g] = 2;
         }
-        group_of[ri] = (uint32_t)(gk0.size() - 1);
+    });
+    if (third < S) {
+        set_error("non-manifold mesh: a face is shared by more than two elements (element " +
+                  std::to_string(srt[third].cell) + ")");
+        return false;
     }
     std::vector<FaceRec>().swap(srt);
     const int64_t F = (int64_t)gk0.size();

@@ -104,6 +104,24 @@ def test_parallel_parse_reports_the_first_bad_element(workdir, first, second, me
     assert message in capi.last_error(), capi.last_error()
 
 
+def test_parallel_builder_rejects_a_face_of_three_elements(workdir):
+    """A 140k-element mesh with one element listed twice: its faces are shared
+    by three elements, which the parallel grouping reports as non-manifold."""
+    from graphite_b200 import meshgen
+    path = str(workdir / "dup.su2")
+    meshgen.channel_bump(nx=60, ny=30, nz=13, cells="tet").write_su2(path)
+    lines = open(path).read().split("\n")
+    at = next(i for i, l in enumerate(lines) if l.startswith("NELEM="))
+    n = int(lines[at].split("=")[1])
+    lines[at] = f"NELEM= {n + 1}"
+    lines.insert(at + 1 + 70000, lines[at + 1 + 70000])
+    with open(path, "w") as f:
+        f.write("\n".join(lines))
+    out = str(workdir / "dup.fvm").encode()
+    assert capi.load().cuMeshFromSu2(path.encode(), out) != 0
+    assert "non-manifold" in capi.last_error(), capi.last_error()
+
+
 def _write(path, text):
     with open(path, "w") as f:
         f.write(text)
