@@ -25,6 +25,7 @@ import os
 import shutil
 import subprocess
 import sys
+import tempfile
 import time
 
 import numpy as np
@@ -62,7 +63,7 @@ def run(args, log):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--out", default=HERE)
-    ap.add_argument("--work", default=os.path.join(ROOT, "gpurun_out", "golden_work"))
+    ap.add_argument("--work", default=os.path.join(tempfile.gettempdir(), "graphite_b200_golden_work"))
     ap.add_argument("--only", default="", help="comma list of metrics,prepare,solve")
     a = ap.parse_args()
     os.makedirs(a.out, exist_ok=True)
