@@ -3,8 +3,8 @@
 //
 // TEST INFRASTRUCTURE, NOT PART OF THE PRODUCT.  Only tests/, the smoke check
 // in __graft_entry__.py and bench.py's CPU-baseline leg load this library
-// (oracle/_build/liboracle.so), and only as the checker / the timed CPU
-// restatement.  The product path (graphite_b200/) never calls it.
+// (oracle/_build/liboracle.so), and only to check results against / as the
+// timed CPU restatement.  The product path (graphite_b200/) never calls it.
 //
 // It restates, function by function, the reference's algorithm in plain C++
 // (templated on float/double, OpenMP over cells):

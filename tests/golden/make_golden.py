@@ -6,8 +6,8 @@ in a tree where the reference sources are present; the built
 
     python tests/golden/make_golden.py --out tests/golden
 
-For each case in cases.py it writes the SU2 mesh, runs the driver in one of
-its modes and stores the arrays as ``<case>_<mode>.npz``:
+For each case in cases.py it writes the SU2 mesh, runs the reference harness
+(oracle/ref_driver.cu) in one of its modes and stores the arrays as ``<case>_<mode>.npz``:
 
 * metrics  - the reference converter's .fvm file (``<case>_ref.fvm``) and
              the reference's mesh arrays after cuMeshFromSu2/cuMeshFromFile

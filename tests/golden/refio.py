@@ -2,7 +2,7 @@
 
 ``read_records`` parses the record stream that oracle/ref_driver.cu writes:
 {char name[64]; uint32 dtype (0 f32, 1 u32, 2 f64, 3 u64); uint64 count; data}.
-``write_case`` writes the driver's plain-text case description.
+``write_case`` writes the harness's plain-text case description.
 """
 from __future__ import annotations
 
