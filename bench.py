@@ -293,23 +293,47 @@ def run_ours(args, rank, world, local_rank):
     traffic = ncu_traffic(dominant, args.workload)
 
     # ---- e2e: the apps/main.cu loop through the C ABI from host buffers ----
+    # The initial state sits in the fields' pinned host mirrors (FvmField
+    # _cpu->value, the buffers a reference caller fills); the timed region
+    # uploads it (gbVarCpuToGpu), runs K iterations of the per-call loop
+    # (boundary conditions, FvmEulerStepPrepare, FvmEulerStep and the
+    # residual read back by FvmFieldReduceSum every iteration) and downloads
+    # the final state into the mirrors (VarGpuToCpu).
     case.init(mach, P_INF, T_INF)
-    rho0, rhou0, rhoe0 = case.fields()     # initial state in pinned host mirrors
+    case.download_mirrors()
     torch.cuda.synchronize()
     if world > 1:
         torch.distributed.barrier()
     te0 = time.perf_counter()
-    case.set_state(rho0, rhou0, rhoe0)     # H2D from the pinned mirrors
+    case.upload_mirrors()                  # H2D from the pinned mirrors
     for _ in range(K):
         case.iterate(bcs, CFL)             # BCs, prepare, step, residual -> host
-    rho1, rhou1, rhoe1 = case.fields()     # D2H of the final state
+    case.download_mirrors()                # D2H of the final state
     te = time.perf_counter() - te0
     te = max_over_ranks(te, world)
-    state_bytes = (rho0.nbytes + rhou0.nbytes + rhoe0.nbytes)
+    state_bytes = case.state_bytes()
+    # the same from the replayed-graph loop (gbEulerRun), the residual read
+    # back to the host after every iteration (check_every = 1)
+    case.init(mach, P_INF, T_INF)
+    case.download_mirrors()
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    tg0 = time.perf_counter()
+    case.upload_mirrors()
+    case.run(bcs, CFL, K, check_every=1)
+    case.download_mirrors()
+    tg = time.perf_counter() - tg0
+    tg = max_over_ranks(tg, world)
     e2e = {"value": whole_job_rate(world, N, K, te), "unit": "cell-updates/s",
            "h2d_bytes_per_step": state_bytes / K, "d2h_bytes_per_step": 8 + state_bytes / K,
-           "path": "per-call C ABI (FvmEuler*Bc, FvmEulerStepPrepare, FvmEulerStep, FvmFieldReduceSum) "
-                   "with the state uploaded from and read back to pinned host memory"}
+           "seconds": te,
+           "path": "per-call C ABI (FvmEuler*Bc, FvmEulerStepPrepare, FvmEulerStep, FvmFieldReduceSum with its "
+                   "residual read back every iteration), the state uploaded from and read back to the fields' "
+                   "pinned host mirrors",
+           "graph_loop": {"value": whole_job_rate(world, N, K, tg), "unit": "cell-updates/s", "seconds": tg,
+                          "path": "gbEulerRun (replayed graphs, residual read back every iteration), same "
+                                  "upload and read-back"}}
 
     # ---- time to a 1e-3 residual drop (reference's squared residual) ----
     ttr = None
@@ -349,10 +373,8 @@ def run_ours(args, rank, world, local_rank):
         "warmup": W, "ms_per_step": t_ms / K, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32 (f64 metrics and reductions)",
         "data": "synthetic procedural mesh and uniform free-stream start",
-        "config": {"workload": args.workload, "description": WORKLOADS[args.workload]["desc"], "cells": N,
-                   "ghosts": case.n_ghosts, "faces": case.n_faces, "cfl": CFL, "parallelism": f"replicas x{world}",
-                   "l2": "inputs larger than L2: %.0f MB resident on the device" % resident_mb(case, bm),
-                   "mesh_setup_seconds": setup_s},
+        "config": bench_config(args.workload, N, case.n_ghosts, case.n_faces, world),
+        "resident_mb": resident_mb(case, bm), "mesh_setup_seconds": setup_s,
         "e2e": e2e,
         "gpu_launches": int(launches),
         "roofline": {"bound": "hbm", "kernel": dominant, "achieved": achieved, "peak": peak,
@@ -371,6 +393,16 @@ def run_ours(args, rank, world, local_rank):
     }
     case.close()
     return out
+
+
+CPU_BLOCK = 65536   # cells per oracle call in the CPU legs
+
+
+def bench_config(workload, cells, ghosts, faces, world):
+    """The `config` object both arms print for the same workload."""
+    return {"workload": workload, "description": WORKLOADS[workload]["desc"], "cells": int(cells),
+            "ghosts": int(ghosts), "faces": int(faces), "cfl": CFL, "parallelism": f"replicas x{world}",
+            "l2": "inputs larger than L2 (the state, face states and mesh arrays: hundreds of MB)"}
 
 
 def resident_mb(case, bm):
@@ -396,7 +428,7 @@ def cpu_baseline(workload, max_seconds=20.0, sample_cells=None):
     s.init(mach, P_INF, T_INF)
     s.apply_bcs(bcs)
     N = om.N
-    block = sample_cells or min(N, 65536)
+    block = sample_cells or min(N, CPU_BLOCK)
     s.sample_step(CFL, 0, block)          # warm-up
     done, t0, c = 0, time.perf_counter(), 0
     while time.perf_counter() - t0 < max_seconds:
@@ -661,8 +693,9 @@ def run_cylinder(args, dev_stream):
     NSICase.set_constants(1.0, 1.0 / 40.0, 2.0, True, False)
     c = NSICase(path)
     base = c.mesh.contents._cpu.contents
+    n_cells = int(base.n_cells)
     cent = np.array([[base.cell_centers[i].x, base.cell_centers[i].y, base.cell_centers[i].z]
-                     for i in range(c.n_cells)])
+                     for i in range(n_cells)])
     span, out = 0.1, {}
     for label, tol, check in (("to_1e-3", 1e-3, 1), ("converged_1e-10", 1e-10, 2000)):
         c.init((1.0, 0.0, 0.0), 0.0)
@@ -683,15 +716,17 @@ def run_cylinder(args, dev_stream):
                       "wake_length_diameters": recirculation_length(cent, u[: c.n_cells]),
                       "residual_ratio": float(r[-1])}
     c.close()
-    return {"mesh": "cylinder O-grid 400 x 250 x 1 hexes, stretching 1.03, far field 30 D", "cells": int(base.n_cells),
+    return {"mesh": "cylinder O-grid 400 x 250 x 1 hexes, stretching 1.03, far field 30 D", "cells": n_cells,
             "reynolds": 40, "beta": 2.0, "cfl": 0.8, "laplacian": "average + compact correction",
             "limiter": "none", **out,
             "published_range": {"drag_coefficient": [1.50, 1.60], "wake_length_diameters": [2.13, 2.35]}}
 
 
 def run_reference(args, rank, world):
-    """The oracle port on the host cores: each step is one bounded sample (a
-    block of cells) of the iteration."""
+    """The oracle port on the host cores (rank 0 only), all host threads:
+    each step is one full iteration over every interior cell of the
+    workload's mesh (gradients, limiters, flux and update), processed in
+    blocks of 65,536 cells as cpu_baseline does."""
     if rank != 0:
         return None
     import oracle.pyoracle as po
@@ -703,29 +738,28 @@ def run_reference(args, rank, world):
     s.init(mach, P_INF, T_INF)
     s.apply_bcs(bcs)
     N = om.N
-    block = min(N, 8192)
-    c = 0
+    block = min(N, CPU_BLOCK)
+
+    def iteration():
+        for c in range(0, N, block):
+            s.sample_step(CFL, c, min(N, c + block))
+
     for _ in range(args.warmup):
-        s.sample_step(CFL, c, min(N, c + block))
-        c = (c + block) % N
+        iteration()
     t0 = time.perf_counter()
-    done = 0
     for _ in range(args.steps):
-        c1 = min(N, c + block)
-        s.sample_step(CFL, c, c1)
-        done += c1 - c
-        c = 0 if c1 >= N else c1
+        iteration()
     dt = time.perf_counter() - t0
-    v = done / dt
+    v = N * args.steps / dt
     ref_gpu = reference_gpu_build(args.workload)
     return {"metric": "cell-updates/s", "value": v, "unit": "cell-updates/s", "impl": "reference",
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3 / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic procedural mesh and uniform free-stream start",
-            "config": {"workload": args.workload, "description": WORKLOADS[args.workload]["desc"], "cells": N,
-                       "parallelism": "host cores", "sample_block_cells": block},
+            "config": bench_config(args.workload, N, om.G, om.F, world),
             "cpu_baseline": {"value": v, "unit": "cell-updates/s", "cores": po.max_threads(), "kind": "port",
-                             "sample": f"{args.steps} blocks of {block} cells (one block per step)"},
+                             "sample": f"{args.steps} full iterations of the {N}-cell mesh in blocks of {block} "
+                                       f"cells over {dt:.1f} s (gradients, limiters, flux and update; float32)"},
             "e2e": {"value": v, "unit": "cell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
             "note": "the reference has no host implementation of this path (all of it is CUDA); this is the "
                     "oracle, a C++ restatement of the reference's kernels, with OpenMP over cells",

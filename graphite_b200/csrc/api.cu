@@ -58,14 +58,46 @@ void dfree(T*& p) {
     p = nullptr;
 }
 
+// The instantiated graphs of a replayed loop (gbEulerRun / gbNSIRun), kept
+// on the mesh between calls.  `key` holds everything the captured launches
+// bake in (field identities and device buffers, CFL, boundary conditions,
+// modes); a call whose key matches replays the graphs without capturing
+// again.  The residual history of one chunk of iterations goes to `hist`
+// (capacity `cap`), the counter is reset before every chunk.
+struct RunGraphs {
+    std::vector<uint64_t> key;
+    cudaGraphExec_t exec[2] = {nullptr, nullptr};
+    double* hist = nullptr;
+    unsigned long long* counter = nullptr;
+    int64_t cap = 0;
+    int per_iter = 0;
+    void release() {
+        for (int k = 0; k < 2; ++k)
+            if (exec[k]) cudaGraphExecDestroy(exec[k]);
+        exec[0] = exec[1] = nullptr;
+        if (hist) cudaFree(hist);
+        if (counter) cudaFree(counter);
+        hist = nullptr;
+        counter = nullptr;
+        cap = 0;
+        key.clear();
+    }
+};
+
 struct MeshImpl {
     Topology topo;
     Numbering num;
     DevMesh dev;
     uint32_t* d_cell_new = nullptr;   // old -> new, N+G
+    RunGraphs euler_run, nsi_run;
+    cudaStream_t capture = nullptr;   // stream the loops are captured on
+    double* h_result = nullptr;       // pinned: FvmFieldReduceSum's value on the host
 };
 
+std::atomic<uint64_t> g_field_ids{0};
+
 struct FieldImpl {
+    uint64_t id = ++g_field_ids;      // never reused: cached graphs refer to a field by it
     int comps = 1;                    // 1 scalar, 3 vector
     size_t size = 0;
     int alloc_grads = 0;
@@ -106,6 +138,10 @@ void free_mesh(cuMesh* m) {
         dfree(d.cell_geo); dfree(d.face_geo); dfree(d.nfc); dfree(d.nb); dfree(d.lsq); dfree(d.ghost); dfree(d.red);
         dfree(d.twin); dfree(d.cf_geo); dfree(d.nbc); dfree(d.dn); dfree(d.df);
         dfree(mi->d_cell_new);
+        mi->euler_run.release();
+        mi->nsi_run.release();
+        if (mi->capture) cudaStreamDestroy(mi->capture);
+        if (mi->h_result) cudaFreeHost(mi->h_result);
         delete mi;
     }
     free_host_mesh(m->_cpu);
@@ -189,7 +225,8 @@ cuMesh* create_mesh(Topology&& topo) {
          dalloc(d.nbc, (size_t)d.S, "alloc mesh") && dalloc(d.dn, (size_t)d.S, "alloc mesh") &&
          dalloc(d.df, (size_t)d.S, "alloc mesh");
     d.n_red_max = std::max<int>(reduce_blocks(NG), (int)((N + kBlock - 1) / kBlock));
-    ok = ok && dalloc(d.red, (size_t)d.n_red_max + 1, "alloc reduction");
+    ok = ok && dalloc(d.red, (size_t)d.n_red_max + 1, "alloc reduction") &&
+         cuda_ok(cudaMallocHost((void**)&mi->h_result, sizeof(double)), "alloc reduction");
     if (ok) {
         launch_layout(d, d_cell_old, d_face_old, area, normal, fcen, ccen, vol, minv, s);
         launch_entry_geo(d, s);
@@ -434,6 +471,95 @@ bool download_gradients(FvmField* f) {
         }
     }
     return true;
+}
+
+// ---- replayed loops (gbEulerRun, gbNSIRun) ----
+
+void key_field(std::vector<uint64_t>& k, const FvmField* f) {
+    const FieldImpl* fi = impl(f);
+    for (uint64_t w : {fi->id, (uint64_t)(uintptr_t)fi->val[0], (uint64_t)(uintptr_t)fi->val[1],
+                       (uint64_t)(uintptr_t)fi->rec, (uint64_t)(uintptr_t)fi->grad,
+                       (uint64_t)(uintptr_t)fi->partials, (uint64_t)fi->n_partials})
+        k.push_back(w);
+}
+
+void key_bytes(std::vector<uint64_t>& k, const void* p, size_t n) {
+    const unsigned char* c = static_cast<const unsigned char*>(p);
+    for (size_t i = 0; i < n; i += 8) {
+        uint64_t w = 0;
+        memcpy(&w, c + i, std::min<size_t>(8, n - i));
+        k.push_back(w);
+    }
+}
+
+// Makes `rg` hold graphs for `key` with a history of at least `need` entries
+// per chunk, capturing them (enqueue(k, stream, hist, counter, cap) for value
+// buffer parity k) only when the key or the capacity changed.
+template <class Enqueue>
+bool ensure_run_graphs(MeshImpl* mi, RunGraphs& rg, std::vector<uint64_t>& key, int64_t need, int per_iter,
+                       Enqueue&& enqueue, const char* what) {
+    if (rg.exec[0] && rg.exec[1] && rg.key == key && rg.cap >= need) return true;
+    const int64_t cap = std::max<int64_t>(need, std::max<int64_t>(256, rg.cap));
+    rg.release();
+    if (!mi->capture && !cuda_ok(cudaStreamCreateWithFlags(&mi->capture, cudaStreamNonBlocking), what)) return false;
+    if (!dalloc(rg.hist, (size_t)cap, what) || !dalloc(rg.counter, 1, what)) { rg.release(); return false; }
+    rg.cap = cap;
+    bool ok = true;
+    t_counting = false;
+    for (int k = 0; k < 2 && ok; ++k) {
+        cudaGraph_t g = nullptr;
+        ok = cuda_ok(cudaStreamBeginCapture(mi->capture, cudaStreamCaptureModeThreadLocal), "graph capture");
+        if (!ok) break;
+        enqueue(k, mi->capture, rg.hist, rg.counter, (unsigned long long)cap);
+        ok = cuda_ok(cudaStreamEndCapture(mi->capture, &g), "graph capture") &&
+             cuda_ok(cudaGraphInstantiate(&rg.exec[k], g, 0), "graph instantiate");
+        if (g) cudaGraphDestroy(g);
+    }
+    t_counting = true;
+    if (!ok) { rg.release(); return false; }
+    rg.key = key;
+    rg.per_iter = per_iter;
+    return true;
+}
+
+// Replays the graphs from value buffer `cur` for up to n_iter iterations,
+// check_every at a time; after each chunk that chunk's residuals come back
+// to `hist` and the loop stops once one of them is below tolerance x the
+// first (tolerance > 0) or is not finite (an error).  Returns the
+// iterations run, or -1; `cur` becomes the buffer holding the last state.
+int64_t replay_run_graphs(RunGraphs& rg, int& cur, int64_t n_iter, int64_t check_every, double tolerance,
+                          std::vector<double>& hist, cudaStream_t s, const char* what) {
+    int64_t done = 0;
+    bool ok = true;
+    while (ok && done < n_iter) {
+        const int64_t chunk = std::min<int64_t>(check_every, n_iter - done);
+        ok = cuda_ok(cudaMemsetAsync(rg.counter, 0, sizeof(unsigned long long), s), what);
+        for (int64_t i = 0; i < chunk && ok; ++i) {
+            ok = cuda_ok(cudaGraphLaunch(rg.exec[cur], s), "graph launch");
+            count_launch(rg.per_iter);
+            cur = 1 - cur;
+        }
+        if (!ok) break;
+        ok = cuda_ok(cudaMemcpyAsync(hist.data() + done, rg.hist, (size_t)chunk * sizeof(double),
+                                     cudaMemcpyDeviceToHost, s), what) &&
+             cuda_ok(cudaStreamSynchronize(s), what);
+        done += chunk;
+        if (!ok) break;
+        bool bad = false;
+        for (int64_t i = done - chunk; i < done; ++i) bad |= !std::isfinite(hist[i]);
+        if (bad) {
+            set_error(std::string(what) + ": residual is not finite (diverged)");
+            ok = false;
+            break;
+        }
+        if (tolerance > 0.0 && hist[0] > 0.0) {
+            bool stop = false;
+            // iterations past the first one below tolerance in this chunk already ran; all are reported
+            for (int64_t i = done - chunk; i < done && !stop; ++i) stop = hist[i] / hist[0] < tolerance;
+            if (stop) break;
+        }
+    }
+    return ok ? done : -1;
 }
 
 }  // namespace
@@ -736,12 +862,14 @@ gb_scalar FvmFieldReduceSum(cuMesh* mesh, FvmField* var) {
         launch_reduce_partials(mi->dev.N, (const float*)fi->val[fi->cur], mi->dev.red, s);
         launch_reduce_final(nb, mi->dev.red, out, nullptr, nullptr, s);
     }
-    double h = 0.0;
+    // read back through a pinned word: a copy into pageable memory would be
+    // staged by the driver
+    double* h = mi->h_result;
     if (!launch_ok("FvmFieldReduceSum") ||
-        !cuda_ok(cudaMemcpyAsync(&h, out, sizeof(double), cudaMemcpyDeviceToHost, s), "FvmFieldReduceSum") ||
+        !cuda_ok(cudaMemcpyAsync(h, out, sizeof(double), cudaMemcpyDeviceToHost, s), "FvmFieldReduceSum") ||
         !cuda_ok(cudaStreamSynchronize(s), "FvmFieldReduceSum"))
         return nan;
-    return (gb_scalar)h;
+    return (gb_scalar)*h;
 }
 
 int64_t gbEulerRun(cuMesh* mesh, FvmField* rho, FvmField* rhou, FvmField* rhoe, FvmField* error, gb_scalar cfl,
@@ -764,13 +892,6 @@ int64_t gbEulerRun(cuMesh* mesh, FvmField* rho, FvmField* rhou, FvmField* rhoe, 
     if (!ensure_partials(ei, std::max(nb, 1))) return -1;
     if (check_every <= 0) check_every = 100;
     cudaStream_t s = t_stream;
-    double* d_hist = nullptr;
-    unsigned long long* d_counter = nullptr;
-    if (!dalloc(d_hist, (size_t)n_iter, "gbEulerRun") || !dalloc(d_counter, 1, "gbEulerRun") ||
-        !cuda_ok(cudaMemsetAsync(d_counter, 0, sizeof(unsigned long long), s), "gbEulerRun")) {
-        dfree(d_hist); dfree(d_counter);
-        return -1;
-    }
     double* out = mi->dev.red + mi->dev.n_red_max;
     // The boundary conditions as a table by ghost region.  On ghost-heavy
     // meshes (one-layer extrusions carry two span ghosts per cell) the
@@ -799,68 +920,39 @@ int64_t gbEulerRun(cuMesh* mesh, FvmField* rho, FvmField* rhou, FvmField* rhoe, 
             gbt.rhoe[k] = (float*)impl(rhoe)->val[k];
         }
     }
+    // what the captured launches bake in
+    const bool transposed = g_transposed.load() != 0;
+    std::vector<uint64_t> key;
+    for (const FvmField* f : {rho, rhou, rhoe, error}) key_field(key, f);
+    key.push_back((uint64_t)ei->cur);
+    key.push_back((uint64_t)transposed);
+    key_bytes(key, &cfl, sizeof(cfl));
+    key.push_back((uint64_t)n_bc);
+    if (n_bc > 0) key_bytes(key, bcs, sizeof(gbBc) * (size_t)n_bc);
     // one graph per value buffer parity: BCs, gradients+limiters, flux+update, residual
-    cudaGraphExec_t exec[2] = {nullptr, nullptr};
-    cudaStream_t cap = nullptr;
-    bool ok = cuda_ok(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking), "gbEulerRun");
-    t_counting = false;
-    for (int k = 0; k < 2 && ok; ++k) {
-        cudaGraph_t g = nullptr;
-        ok = cuda_ok(cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal), "graph capture");
-        if (!ok) break;
+    auto enqueue = [&](int k, cudaStream_t cap, double* hist, unsigned long long* counter, unsigned long long hcap) {
         if (table_bcs && !inline_bcs && n_bc > 0) launch_bc_table(mi->dev, gbt, k, cap);
         for (int b = 0; b < n_bc && !table_bcs; ++b) {
             if (bcs[b].type == 0) enqueue_slip(mesh, rho, rhou, rhoe, (int)bcs[b].region_id, k, cap);
             else enqueue_farfield(mesh, rho, rhou, rhoe, (int)bcs[b].region_id, k, bcs[b].mach, bcs[b].pressure,
                                   bcs[b].temperature, cap);
         }
-        launch_grad_lim(mi->dev, state_of(rho, rhou, rhoe, k), grad_of(rho, rhou, rhoe, false),
-                        g_transposed.load() != 0, cap, inline_bcs ? &gbt : nullptr);
+        launch_grad_lim(mi->dev, state_of(rho, rhou, rhoe, k), grad_of(rho, rhou, rhoe, false), transposed, cap,
+                        inline_bcs ? &gbt : nullptr);
         enqueue_flux(mesh, rho, rhou, rhoe, error, cfl, k, cap);
-        launch_reduce_final(nb, ei->partials, out, d_hist, d_counter, cap);
-        ok = cuda_ok(cudaStreamEndCapture(cap, &g), "graph capture") &&
-             cuda_ok(cudaGraphInstantiate(&exec[k], g, 0), "graph instantiate");
-        if (g) cudaGraphDestroy(g);
-    }
-    t_counting = true;
+        launch_reduce_final(nb, ei->partials, out, hist, counter, cap, hcap);
+    };
     const int per_iter = (inline_bcs ? 0 : (table_bcs ? (n_bc > 0 ? 1 : 0) : n_bc)) + 3;
+    if (!ensure_run_graphs(mi, mi->euler_run, key, std::min<int64_t>(check_every, n_iter), per_iter, enqueue,
+                           "gbEulerRun"))
+        return -1;
     int cur = impl(rho)->cur;
-    int64_t done = 0;
     std::vector<double> hist((size_t)n_iter, 0.0);
-    while (ok && done < n_iter) {
-        const int64_t chunk = std::min<int64_t>(check_every, n_iter - done);
-        for (int64_t i = 0; i < chunk && ok; ++i) {
-            ok = cuda_ok(cudaGraphLaunch(exec[cur], s), "graph launch");
-            count_launch(per_iter);
-            cur = 1 - cur;
-        }
-        done += chunk;
-        if (!ok) break;
-        ok = cuda_ok(cudaMemcpyAsync(hist.data(), d_hist, done * sizeof(double), cudaMemcpyDeviceToHost, s), "gbEulerRun") &&
-             cuda_ok(cudaStreamSynchronize(s), "gbEulerRun");
-        if (ok && tolerance > 0.0 && hist[0] > 0.0) {
-            int64_t stop = -1;
-            for (int64_t i = done - chunk; i < done; ++i)
-                if (hist[i] / hist[0] < tolerance) { stop = i + 1; break; }
-            if (stop > 0) {
-                // iterations past `stop` in this chunk already ran; report all of them
-                break;
-            }
-        }
-        if (ok) {
-            bool bad = false;
-            for (int64_t i = done - chunk; i < done; ++i) bad |= !std::isfinite(hist[i]);
-            if (bad) { set_error("gbEulerRun: residual is not finite (diverged)"); ok = false; }
-        }
-    }
+    const int64_t done = replay_run_graphs(mi->euler_run, cur, n_iter, check_every, tolerance, hist, s, "gbEulerRun");
     impl(rho)->cur = impl(rhou)->cur = impl(rhoe)->cur = cur;
     ei->partials_valid = true;
-    if (residual_history) memcpy(residual_history, hist.data(), (size_t)done * sizeof(double));
-    for (int k = 0; k < 2; ++k) if (exec[k]) cudaGraphExecDestroy(exec[k]);
-    if (cap) cudaStreamDestroy(cap);
-    dfree(d_hist);
-    dfree(d_counter);
-    return ok ? done : -1;
+    if (residual_history && done > 0) memcpy(residual_history, hist.data(), (size_t)done * sizeof(double));
+    return done;
 }
 
 }  // extern "C"
@@ -1041,13 +1133,6 @@ int64_t gbNSIRun(cuMesh* mesh, FvmField* velocity, FvmField* pressure, FvmField*
     if (!ensure_partials(ei, std::max(nb, 1))) return -1;
     if (check_every <= 0) check_every = 100;
     cudaStream_t s = t_stream;
-    double* d_hist = nullptr;
-    unsigned long long* d_counter = nullptr;
-    if (!dalloc(d_hist, (size_t)n_iter, "gbNSIRun") || !dalloc(d_counter, 1, "gbNSIRun") ||
-        !cuda_ok(cudaMemsetAsync(d_counter, 0, sizeof(unsigned long long), s), "gbNSIRun")) {
-        dfree(d_hist); dfree(d_counter);
-        return -1;
-    }
     double* out = mi->dev.red + mi->dev.n_red_max;
     // On ghost-heavy meshes (one-layer extrusions carry two span ghosts per
     // cell) the gradient kernel applies the boundary conditions itself
@@ -1071,59 +1156,32 @@ int64_t gbNSIRun(cuMesh* mesh, FvmField* velocity, FvmField* pressure, FvmField*
             gt.u[k] = (float4*)impl(velocity)->val[k];
         }
     }
-    cudaGraphExec_t exec[2] = {nullptr, nullptr};
-    cudaStream_t cap = nullptr;
-    bool ok = cuda_ok(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking), "gbNSIRun");
-    t_counting = false;
-    for (int k = 0; k < 2 && ok; ++k) {
-        cudaGraph_t g = nullptr;
-        ok = cuda_ok(cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal), "graph capture");
-        if (!ok) break;
+    std::vector<uint64_t> key;
+    for (const FvmField* f : {velocity, pressure, error}) key_field(key, f);
+    key.push_back((uint64_t)ei->cur);
+    key_bytes(key, &cfl, sizeof(cfl));
+    key.push_back((uint64_t)n_bc);
+    if (n_bc > 0) key_bytes(key, bcs, sizeof(gbBc) * (size_t)n_bc);
+    key_bytes(key, &t_nsi, sizeof(t_nsi));
+    auto enqueue = [&](int k, cudaStream_t cap, double* hist, unsigned long long* counter, unsigned long long hcap) {
         for (int b = 0; b < n_bc && !inline_bcs; ++b) {
             const int type = bcs[b].type == 1 ? 1 : (bcs[b].type == 2 ? 2 : 0);
             enqueue_nsi_bc(mesh, velocity, pressure, (int)bcs[b].region_id, type, k, bcs[b].mach, bcs[b].pressure, cap);
         }
         enqueue_nsi_step(mesh, velocity, pressure, error, cfl, k, cap, inline_bcs ? &gt : nullptr);
-        launch_reduce_final(nb, ei->partials, out, d_hist, d_counter, cap);
-        ok = cuda_ok(cudaStreamEndCapture(cap, &g), "graph capture") &&
-             cuda_ok(cudaGraphInstantiate(&exec[k], g, 0), "graph instantiate");
-        if (g) cudaGraphDestroy(g);
-    }
-    t_counting = true;
+        launch_reduce_final(nb, ei->partials, out, hist, counter, cap, hcap);
+    };
     const int per_iter = (inline_bcs ? 0 : n_bc) + 3;
+    if (!ensure_run_graphs(mi, mi->nsi_run, key, std::min<int64_t>(check_every, n_iter), per_iter, enqueue,
+                           "gbNSIRun"))
+        return -1;
     int cur = impl(pressure)->cur;
-    int64_t done = 0;
     std::vector<double> hist((size_t)n_iter, 0.0);
-    while (ok && done < n_iter) {
-        const int64_t chunk = std::min<int64_t>(check_every, n_iter - done);
-        for (int64_t i = 0; i < chunk && ok; ++i) {
-            ok = cuda_ok(cudaGraphLaunch(exec[cur], s), "graph launch");
-            count_launch(per_iter);
-            cur = 1 - cur;
-        }
-        done += chunk;
-        if (!ok) break;
-        ok = cuda_ok(cudaMemcpyAsync(hist.data(), d_hist, done * sizeof(double), cudaMemcpyDeviceToHost, s), "gbNSIRun") &&
-             cuda_ok(cudaStreamSynchronize(s), "gbNSIRun");
-        if (ok && tolerance > 0.0 && hist[0] > 0.0) {
-            bool stop = false;
-            for (int64_t i = done - chunk; i < done && !stop; ++i) stop = hist[i] / hist[0] < tolerance;
-            if (stop) break;
-        }
-        if (ok) {
-            bool bad = false;
-            for (int64_t i = done - chunk; i < done; ++i) bad |= !std::isfinite(hist[i]);
-            if (bad) { set_error("gbNSIRun: residual is not finite (diverged)"); ok = false; }
-        }
-    }
+    const int64_t done = replay_run_graphs(mi->nsi_run, cur, n_iter, check_every, tolerance, hist, s, "gbNSIRun");
     impl(velocity)->cur = impl(pressure)->cur = cur;
     ei->partials_valid = true;
-    if (residual_history) memcpy(residual_history, hist.data(), (size_t)done * sizeof(double));
-    for (int k = 0; k < 2; ++k) if (exec[k]) cudaGraphExecDestroy(exec[k]);
-    if (cap) cudaStreamDestroy(cap);
-    dfree(d_hist);
-    dfree(d_counter);
-    return ok ? done : -1;
+    if (residual_history && done > 0) memcpy(residual_history, hist.data(), (size_t)done * sizeof(double));
+    return done;
 }
 
 int gbNSIWallForce(cuMesh* mesh, FvmField* velocity, FvmField* pressure, unsigned region_id, double* force) {

@@ -174,7 +174,7 @@ __global__ void k_reduce_partials(int64_t n, const float* __restrict__ v, double
 }
 
 __global__ void k_reduce_final(int n, const double* __restrict__ partials, double* out, double* history,
-                               unsigned long long* counter) {
+                               unsigned long long* counter, unsigned long long history_cap) {
     double s = 0.0;
     for (int i = threadIdx.x; i < n; i += blockDim.x) s += partials[i];
     const double bs = block_sum(s);
@@ -182,7 +182,7 @@ __global__ void k_reduce_final(int n, const double* __restrict__ partials, doubl
         out[0] = bs;
         if (history) {
             const unsigned long long it = *counter;
-            history[it] = bs;
+            if (it < history_cap) history[it] = bs;
             *counter = it + 1;
         }
     }
@@ -296,8 +296,8 @@ void launch_reduce_partials_blocks(int64_t n, const float* v, double* partials, 
 }
 
 void launch_reduce_final(int n_partials, const double* partials, double* out, double* history,
-                         unsigned long long* counter, cudaStream_t s) {
-    k_reduce_final<<<1, kBlock, 0, s>>>(n_partials, partials, out, history, counter);
+                         unsigned long long* counter, cudaStream_t s, unsigned long long history_cap) {
+    k_reduce_final<<<1, kBlock, 0, s>>>(n_partials, partials, out, history, counter, history_cap);
     count_launch();
 }
 

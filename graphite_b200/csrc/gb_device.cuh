@@ -144,8 +144,10 @@ void launch_flux(const DevMesh& m, EulerState q, FaceRecs r, float* rho_n, float
 void launch_reduce_partials(int64_t n, const float* v, double* partials, cudaStream_t s);
 // stage 1 with a caller-chosen number of blocks (one partial per block)
 void launch_reduce_partials_blocks(int64_t n, const float* v, double* partials, int blocks, cudaStream_t s);
+// history (may be null): out[0] is also written to history[*counter] when
+// *counter < history_cap, and *counter is incremented
 void launch_reduce_final(int n_partials, const double* partials, double* out, double* history,
-                         unsigned long long* counter, cudaStream_t s);
+                         unsigned long long* counter, cudaStream_t s, unsigned long long history_cap = 0);
 
 // permute helpers for host transfers (new <-> reference order)
 void launch_gather_scalar(int64_t n, const float* src, const uint32_t* idx, float* dst, cudaStream_t s);

@@ -79,6 +79,24 @@ class EulerCase:
             capi.set_field_values(f, v)
             capi.check(self.lib.gbVarCpuToGpu(self.mesh, f), "gbVarCpuToGpu")
 
+    def upload_mirrors(self) -> None:
+        """gbVarCpuToGpu of rho, rhou and rhoe: the device state becomes what
+        their pinned host mirrors (FvmField _cpu->value) hold."""
+        for f in (self.rho, self.rhou, self.rhoe):
+            capi.check(self.lib.gbVarCpuToGpu(self.mesh, f), "gbVarCpuToGpu")
+
+    def download_mirrors(self) -> None:
+        """VarGpuToCpu of rho, rhou and rhoe into their pinned host mirrors."""
+        for f in (self.rho, self.rhou, self.rhoe):
+            self.lib.VarGpuToCpu(f)
+            if capi.last_error():
+                raise capi.GraphiteError(capi.last_error())
+
+    def state_bytes(self) -> int:
+        """Bytes of the host mirrors of rho, rhou and rhoe (cells and ghosts)."""
+        n = self.n_cells + self.n_ghosts
+        return n * (4 + 12 + 4)
+
     def apply_bcs(self, bcs) -> None:
         for b in bcs:
             if b[0] == "slip":
