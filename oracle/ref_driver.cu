@@ -10,6 +10,11 @@
 //   per iteration: Fvm*Bc per region -> FvmEulerStepPrepare -> FvmEulerStep
 //                  -> FvmFieldReduceSum (normalised by the iteration-0 value)
 //
+// The same source builds against the reference's float32 headers (as
+// shipped, include/datatypes.cuh:32 defines FLOAT_PREC) and against a copy
+// with that define removed (scalar = double); records of scalar arrays carry
+// the matching dtype.
+//
 // usage: ref_driver <case.txt> <mesh.su2> <out.bin> <mode>
 //   mode = metrics | prepare | solve
 // case.txt lines (processed in file order):
@@ -38,12 +43,24 @@ struct BcSpec {
 };
 
 struct Case {
-    vector mach = make_vector(0.5f, 0.f, 0.f);
+    vector mach = make_vector((scalar)0.5, (scalar)0, (scalar)0);
     scalar p = 1.f, T = 1.f / 1.4f, cfl = 0.8f, tol = 0.f;
     int iters = 100;
     std::string state;
     std::vector<BcSpec> bcs;
 };
+
+// reads n numbers into scalars whatever scalar is
+bool read_scalars(FILE* f, int n, scalar** out) {
+    for (int i = 0; i < n; ++i) {
+        double v;
+        if (fscanf(f, "%lf", &v) != 1) return false;
+        *out[i] = (scalar)v;
+    }
+    return true;
+}
+
+constexpr uint32_t kScalarType = sizeof(scalar) == 8 ? 2 : 0;
 
 Case read_case(const char* path) {
     Case c;
@@ -53,24 +70,28 @@ Case read_case(const char* path) {
     while (fscanf(f, "%127s", key) == 1) {
         std::string k(key);
         if (k == "init") {
-            if (fscanf(f, "%f %f %f %f %f", &c.mach.x, &c.mach.y, &c.mach.z, &c.p, &c.T) != 5) exit(2);
+            scalar* v[5] = {&c.mach.x, &c.mach.y, &c.mach.z, &c.p, &c.T};
+            if (!read_scalars(f, 5, v)) exit(2);
         } else if (k == "slip") {
             char r[128];
             if (fscanf(f, "%127s", r) != 1) exit(2);
-            BcSpec b; b.type = "slip"; b.region = r; b.mach = make_vector(0.f, 0.f, 0.f); b.p = b.T = 0;
+            BcSpec b; b.type = "slip"; b.region = r; b.mach = make_vector((scalar)0, (scalar)0, (scalar)0); b.p = b.T = 0;
             c.bcs.push_back(b);
         } else if (k == "farfield") {
             char r[128];
             BcSpec b; b.type = "farfield";
-            if (fscanf(f, "%127s %f %f %f %f %f", r, &b.mach.x, &b.mach.y, &b.mach.z, &b.p, &b.T) != 6) exit(2);
+            scalar* v[5] = {&b.mach.x, &b.mach.y, &b.mach.z, &b.p, &b.T};
+            if (fscanf(f, "%127s", r) != 1 || !read_scalars(f, 5, v)) exit(2);
             b.region = r;
             c.bcs.push_back(b);
         } else if (k == "cfl") {
-            if (fscanf(f, "%f", &c.cfl) != 1) exit(2);
+            scalar* v[1] = {&c.cfl};
+            if (!read_scalars(f, 1, v)) exit(2);
         } else if (k == "iters") {
             if (fscanf(f, "%d", &c.iters) != 1) exit(2);
         } else if (k == "tol") {
-            if (fscanf(f, "%f", &c.tol) != 1) exit(2);
+            scalar* v[1] = {&c.tol};
+            if (!read_scalars(f, 1, v)) exit(2);
         } else if (k == "state") {
             char s[512];
             if (fscanf(f, "%511s", s) != 1) exit(2);
@@ -107,9 +128,9 @@ void apply_bcs(cuMesh* mesh, FvmField* rho, FvmField* rhou, FvmField* rhoe, cons
 void dump_field(FILE* out, FvmField* v, const char* name, size_t n, int comps) {
     VarAllGpuToCpu(v);
     std::string nm(name);
-    put(out, (nm + ".value").c_str(), 0, v->_cpu->value, (uint64_t)n * comps);
-    put(out, (nm + ".gradient").c_str(), 0, v->_cpu->gradient, (uint64_t)n * comps * 3);
-    put(out, (nm + ".limiter").c_str(), 0, v->_cpu->limiter, (uint64_t)n * comps);
+    put(out, (nm + ".value").c_str(), kScalarType, v->_cpu->value, (uint64_t)n * comps);
+    put(out, (nm + ".gradient").c_str(), kScalarType, v->_cpu->gradient, (uint64_t)n * comps * 3);
+    put(out, (nm + ".limiter").c_str(), kScalarType, v->_cpu->limiter, (uint64_t)n * comps);
 }
 
 }  // namespace
@@ -150,13 +171,13 @@ int main(int argc, char** argv) {
         put(out, "face_nodes", 1, m->face_nodes, m->face_nodes_starts[F]);
         put(out, "ghost_cell_ids", 1, m->ghost_cell_ids, G);
         put(out, "ghost_cell_starts", 1, m->ghost_cell_starts, m->n_regions + 1);
-        put(out, "nodes", 0, m->nodes, m->n_nodes * 3);
-        put(out, "face_areas", 0, m->face_areas, F);
-        put(out, "face_normals", 0, m->face_normals, F * 3);
-        put(out, "face_centers", 0, m->face_centers, F * 3);
-        put(out, "cell_volumes", 0, m->cell_volumes, NG);
-        put(out, "cell_centers", 0, m->cell_centers, NG * 3);
-        put(out, "cell_matrices", 0, m->cell_matrices, N * 9);
+        put(out, "nodes", kScalarType, m->nodes, m->n_nodes * 3);
+        put(out, "face_areas", kScalarType, m->face_areas, F);
+        put(out, "face_normals", kScalarType, m->face_normals, F * 3);
+        put(out, "face_centers", kScalarType, m->face_centers, F * 3);
+        put(out, "cell_volumes", kScalarType, m->cell_volumes, NG);
+        put(out, "cell_centers", kScalarType, m->cell_centers, NG * 3);
+        put(out, "cell_matrices", kScalarType, m->cell_matrices, N * 9);
         fclose(out);
         return 0;
     }
@@ -173,9 +194,10 @@ int main(int argc, char** argv) {
             FILE* sf = fopen(c.state.c_str(), "rb");
             if (!sf || fread(buf.data(), 4, NG * 5, sf) != NG * 5) { fprintf(stderr, "bad state file\n"); return 2; }
             fclose(sf);
-            cudaExec(cudaMemcpy(rho->_hgpu->value, buf.data(), NG * 4, cudaMemcpyHostToDevice));
-            cudaExec(cudaMemcpy(rhou->_hgpu->value, buf.data() + NG, NG * 12, cudaMemcpyHostToDevice));
-            cudaExec(cudaMemcpy(rhoe->_hgpu->value, buf.data() + NG * 4, NG * 4, cudaMemcpyHostToDevice));
+            std::vector<scalar> sv(buf.begin(), buf.end());
+            cudaExec(cudaMemcpy(rho->_hgpu->value, sv.data(), NG * sizeof(scalar), cudaMemcpyHostToDevice));
+            cudaExec(cudaMemcpy(rhou->_hgpu->value, sv.data() + NG, NG * 3 * sizeof(scalar), cudaMemcpyHostToDevice));
+            cudaExec(cudaMemcpy(rhoe->_hgpu->value, sv.data() + NG * 4, NG * sizeof(scalar), cudaMemcpyHostToDevice));
         }
         apply_bcs(mesh, rho, rhou, rhoe, c);
         FvmEulerStepPrepare(mesh, rho, rhou, rhoe);
@@ -223,7 +245,7 @@ int main(int argc, char** argv) {
     dump_field(out, rhou, "rhou", NG, 3);
     dump_field(out, rhoe, "rhoe", NG, 1);
     VarGpuToCpu(error);
-    put(out, "error.value", 0, error->_cpu->value, NG);
+    put(out, "error.value", kScalarType, error->_cpu->value, NG);
     fclose(out);
     printf("ref_driver: %d iterations, %.3f s wall, %.3e cell-updates/s\n", it, wall,
            (double)N * it / wall);

@@ -1,7 +1,16 @@
 """The FP32 solver against an FP64 oracle run of the same scheme on the
 benchmark meshes: the transonic swept wing (1.1 M prisms) and the 120k
 airfoil, each from free stream to the 1e-3 drop of the squared residual.
-States the density L2 error and the lift/drag errors."""
+States the density L2 error and the lift/drag errors.
+
+The target for lift and drag is 1e-4 relative.  At this stopping rule the
+FP64 oracle does not reproduce itself to that level: one unit in the last
+place of the initial density moves its lift by 1e-3..5e-3 on the small
+airfoil (tests/test_fp64_floor.py) and by 4e-4 on the 120k airfoil, because
+the limited scheme's residual stalls near the 1e-3 drop.  The bounds below
+are therefore set just above what this build achieves (wing 8e-5 / 3e-5,
+120k airfoil 4.8e-4 / 4.5e-4), and the small-airfoil test compares the FP32
+error with the FP64 spread measured on the same cases."""
 import math
 
 import numpy as np
@@ -48,7 +57,7 @@ def test_swept_wing_to_1e3_against_fp64(workdir):
     print(f"swept wing, {n_it} iterations: FP64 residual ratio {r64:.3e}, rho L2 {l2:.2e}, "
           f"lift {v[0]:.6e} vs {v[1]:.6e} ({el:.2e}), drag {v[2]:.6e} vs {v[3]:.6e} ({ed:.2e})")
     assert r64 < 1.2e-3
-    assert l2 < 2e-4 and el < 2e-3 and ed < 1e-2
+    assert l2 < 2e-4 and el < 5e-4 and ed < 5e-4
 
 
 def test_airfoil_120k_to_1e3_against_fp64(workdir):
@@ -62,4 +71,32 @@ def test_airfoil_120k_to_1e3_against_fp64(workdir):
     print(f"airfoil 120k, {n_it} iterations: FP64 residual ratio {r64:.3e}, rho L2 {l2:.2e}, "
           f"lift {v[0]:.6e} vs {v[1]:.6e} ({el:.2e}), drag {v[2]:.6e} vs {v[3]:.6e} ({ed:.2e})")
     assert r64 < 1.5e-3
-    assert l2 < 1e-4 and el < 2e-3 and ed < 2e-2
+    assert l2 < 1e-4 and el < 1e-3 and ed < 1e-3
+
+
+@pytest.mark.parametrize("mach_m,aoa", [(0.6, 2.5), (0.5, 3.0), (0.75, 3.0), (0.4, -2.0)])
+def test_small_airfoil_fp32_error_within_fp64_spread(workdir, mach_m, aoa):
+    """The FP32 GPU solve against the FP64 oracle, each stopped at its own
+    first iteration below the 1e-3 drop, compared with how far the FP64
+    oracle moves when its initial density is perturbed by one ulp."""
+    from test_fp64_floor import airfoil_bcs, solve_to_drop
+
+    em = meshgen.airfoil_2d_prisms(96, 24)
+    path = str(workdir / "floor_airfoil.su2")
+    em.write_su2(path)
+    mach, bcs = airfoil_bcs(mach_m, aoa)
+    capi.load().gbSetReferenceMomentumReconstruction(1)
+    with EulerCase(path) as c:
+        c.init(mach, cases.P_INF, cases.T_INF)
+        h = c.run(bcs, 0.5, 20000, tolerance=1e-3, check_every=1)
+        l32, d32 = pyoracle.lift_drag(c.wall_force("wing"), mach)
+    om = pyoracle.OracleMesh(em)
+    base = solve_to_drop(om, mach, bcs)
+    pert = [solve_to_drop(om, mach, bcs, perturb_seed=k) for k in (1, 2)]
+    lift = abs(base[1])
+    floor = max(max(abs(p[1] - base[1]), abs(p[2] - base[2])) for p in pert) / lift
+    el, ed = abs(l32 - base[1]) / lift, abs(d32 - base[2]) / lift
+    print(f"M {mach_m} AoA {aoa}: FP32 stops at {len(h)}, FP64 at {base[0]} ({[p[0] for p in pert]}); "
+          f"lift {el:.2e}, drag {ed:.2e} of lift; FP64 spread {floor:.2e}")
+    assert abs(len(h) - base[0]) <= 20
+    assert max(el, ed) <= 3.0 * floor
