@@ -139,6 +139,8 @@ _PROTOS = {
                                      C.c_float]),
     "gbWarmStartGradient": (C.c_int, [C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "gbWarmStartForward": (C.c_int, [C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p]),
+    "gbWarmStartSetWaitLimit": (C.c_int, [C.c_void_p, C.c_longlong]),
+    "gbBatchInjectBarrierFault": (C.c_int, [C.c_void_p]),
     "gbBatchFree": (None, [C.c_void_p]),
     "gbBatchInitUniform": (C.c_int, [C.c_void_p, C.c_int, gb_vector, C.c_float, C.c_float]),
     "gbBatchSetState": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]),

@@ -101,14 +101,18 @@ __device__ __forceinline__ BatchGhostBcs batch_ghosts(const InstDev& I, const Me
                          {I.rhoe[0], I.rhoe[1]}};
 }
 
-// Three forms of the batched gradient / flux kernels: variant 0 and 1 are
-// two register budgets (resident 256-thread blocks per SM; 1 trades a few
-// spills for one more resident block), variant 2 runs the gradient pass in
-// 64-thread blocks that stage each cell's per-face entries in shared memory
-// with cp.async (flux as in variant 1).  The autotuner picks one.
+// Four forms of the batched iteration: variant 0 and 1 are two register
+// budgets of the gradient / flux kernels (resident 256-thread blocks per SM;
+// 1 trades a few spills for one more resident block), variant 2 runs the
+// gradient pass in 64-thread blocks that stage each cell's per-face entries
+// in shared memory with cp.async (flux as in variant 1), and variants 3 and 4
+// are the persistent kernel (k_batch_persistent), which runs a whole chunk of
+// iterations in one cooperative launch, budgeted for 4 or 3 resident
+// 256-thread blocks per SM.  The autotuner picks one.
 constexpr int kBatchGradBlocks[2] = {4, 5};
 constexpr int kBatchFluxBlocks[2] = {4, 5};
-constexpr int kBatchVariants = 3;
+constexpr int kBatchVariants = 5;
+constexpr int kPersistentVariant = 3;     // 3 and 4
 constexpr int kStagedThreads = 64;
 constexpr int kStagedBlocks = 14;
 
@@ -205,6 +209,172 @@ __global__ void k_batch_reduce(InstDev* insts, double tol) {
     }
 }
 
+// ---------------------------------------------------------------------------
+// The persistent form: one cooperative launch runs many iterations of all
+// instances, its three phases (gradients with the boundary conditions, flux
+// + update, per-instance residual) separated by grid-wide barriers instead
+// of kernel boundaries.  Blocks take work items from a counter (an instance
+// that has stopped leaves its items to be skipped), so the last running
+// instances spread over all blocks.  Data that the launch itself writes and
+// reads again after a barrier (states, face states, partial sums, the
+// instance table) is read from L2 (LdCg); the mesh arrays stay on the
+// read-only path.
+struct GridSync {
+    unsigned int count;            // blocks arrived at the current barrier
+    unsigned int gen;              // barrier generation
+    int error;                     // 1: a barrier wait gave up
+    unsigned int pad;
+    unsigned long long grabs[2];   // work-item counters of the two cell phases
+};
+
+constexpr int kPersistThreads = 256;
+constexpr long long kBarrierSpinLimit = 1ll << 22; // a few seconds of polling with back-off
+
+__device__ __forceinline__ unsigned int ld_acquire_u32(const unsigned int* p) {
+    unsigned int v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];\n" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+// Sense-counting grid barrier.  Every block's writes before it are visible to
+// every block after it.  A wait is bounded: after spin_limit polls (or
+// once another block has given up) it sets the error flag and returns false,
+// and the caller leaves the kernel; the host reads the flag.  The cooperative
+// launch guarantees all blocks are resident, so in normal operation every
+// wait ends when the last block arrives.
+__device__ bool grid_barrier(GridSync* gs, long long spin_limit) {
+    __shared__ int s_ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int ok = 1;
+        const unsigned int g = ld_acquire_u32(&gs->gen);
+        __threadfence();
+        if (atomicAdd(&gs->count, 1u) + 1u == gridDim.x) {
+            atomicExch(&gs->count, 0u);
+            __threadfence();
+            atomicAdd(&gs->gen, 1u);
+        } else {
+            long long spins = 0;
+            while (ld_acquire_u32(&gs->gen) == g) {
+                if (++spins > spin_limit || *(volatile int*)&gs->error) {
+                    atomicExch(&gs->error, 1);
+                    ok = 0;
+                    break;
+                }
+                __nanosleep(128);
+            }
+        }
+        __threadfence();
+        s_ok = ok;
+    }
+    __syncthreads();
+    return s_ok != 0;
+}
+
+// Next work item of phase `ph` in iteration `it` of this launch, or n_items
+// when the phase's items are all taken.  Each block takes items until it
+// draws one past the end, so a phase of one iteration draws exactly
+// n_items + gridDim.x times: the counter never needs resetting.
+__device__ __forceinline__ int grab_item(GridSync* gs, int ph, int it, int n_items) {
+    __shared__ int s_item;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const unsigned long long base = (unsigned long long)it * (unsigned long long)(n_items + gridDim.x);
+        const unsigned long long k = atomicAdd(&gs->grabs[ph], 1ull) - base;
+        s_item = k < (unsigned long long)n_items ? (int)k : n_items;
+    }
+    __syncthreads();
+    return s_item;
+}
+
+// BLOCKS: resident blocks per SM the registers are budgeted for
+template <bool TRANSPOSED, int BLOCKS>
+__global__ void __launch_bounds__(kPersistThreads, BLOCKS)
+    k_batch_persistent(const int2* __restrict__ items, int n_items, InstDev* insts, int n_inst,
+                       const MeshTab* __restrict__ meshes, int tile, const BcDev* __restrict__ bcs, float cfl,
+                       double tol, int iters, GridSync* gs, long long spin_limit) {
+    constexpr int B = kPersistThreads;
+    extern __shared__ float4 s_stage[];            // per thread and slot: dn, df, neighbour
+    float4* s_dn = s_stage;
+    float4* s_df = s_stage + kSlots * B;
+    uint32_t* s_nbc = reinterpret_cast<uint32_t*>(s_stage + 2 * kSlots * B);
+    const uint32_t tid = threadIdx.x;
+    for (int it = 0; it < iters; ++it) {
+        // phase 0: gradients, limiters, face states (boundary conditions applied inside)
+        for (;;) {
+            const int k = grab_item(gs, 0, it, n_items);
+            if (k >= n_items) break;
+            const int2 w = items[k];
+            const InstDev& I = insts[w.x];
+            if (__ldcg(&I.status)) continue;           // uniform over the block
+            const MeshTab& M = meshes[I.mesh];
+            const MeshDev m = M.m;
+            const BatchGhostBcs gh = batch_ghosts(I, M, bcs);
+            const int cur = __ldcg(&I.cur);
+            const EulerState q{I.rho[cur], I.rhou[cur], I.rhoe[cur]};
+            const EulerGrad g{nullptr, nullptr, nullptr, I.rec_rho, I.rec_rhou};
+            const uint32_t c0 = (uint32_t)w.y * tile;
+            const uint32_t c1 = min(m.N, c0 + (uint32_t)tile);
+            for (uint32_t i = c0 + tid; i < c1; i += B) {
+                const uint32_t nf = __ldg(&m.nfc[i]);
+                for (uint32_t t = 0; t < nf; ++t) {
+                    const uint32_t e = i + t * m.N;
+                    cp_async4(&s_nbc[t * B + tid], &m.nbc[e]);
+                    cp_async16(&s_dn[t * B + tid], &m.dn[e]);
+                    cp_async16(&s_df[t * B + tid], &m.df[e]);
+                }
+                asm volatile("cp.async.commit_group;\n" ::: "memory");
+                grad_lim_cell<TRANSPOSED, EntriesStaged<B>, BatchGhostBcs, LdCg>(
+                    m, q, g, i, nf, EntriesStaged<B>{s_nbc + tid, s_dn + tid, s_df + tid}, gh);
+            }
+        }
+        if (!grid_barrier(gs, spin_limit)) return;
+        // phase 1: flux, update into the other buffer, partial residual per tile
+        for (;;) {
+            const int k = grab_item(gs, 1, it, n_items);
+            if (k >= n_items) break;
+            const int2 w = items[k];
+            const InstDev& I = insts[w.x];
+            if (__ldcg(&I.status)) continue;
+            const MeshDev m = meshes[I.mesh].m;
+            const int cur = __ldcg(&I.cur), nxt = 1 - cur;
+            const EulerState q{I.rho[cur], I.rhou[cur], I.rhoe[cur]};
+            const uint32_t c0 = (uint32_t)w.y * tile;
+            const uint32_t c1 = min(m.N, c0 + (uint32_t)tile);
+            double res = 0.0;
+            for (uint32_t i = c0 + tid; i < c1; i += B)
+                res += (double)flux_cell<LdCg>(m, q, FaceRecs{I.rec_rho, I.rec_rhou}, I.rho[nxt], I.rhou[nxt],
+                                               I.rhoe[nxt], nullptr, cfl, i);
+            const double bs = block_sum(res);
+            if (tid == 0) I.partials[w.y] = bs;
+        }
+        if (!grid_barrier(gs, spin_limit)) return;
+        // phase 2: per-instance residual, ratio, buffer flip, stop test
+        // (k_batch_reduce's arithmetic; an instance always goes to the same block)
+        for (int k = blockIdx.x; k < n_inst; k += gridDim.x) {
+            __syncthreads();                           // block_sum's scratch is reused
+            InstDev& I = insts[k];
+            if (__ldcg(&I.status)) continue;
+            const int n_tiles = I.n_tiles;
+            double s = 0.0;
+            for (int t = tid; t < n_tiles; t += B) s += __ldcg(&I.partials[t]);
+            const double bs = block_sum(s);
+            if (tid == 0) {
+                if (I.iters == 0) I.res0 = I.res0_fixed > 0.0 ? I.res0_fixed : bs;
+                const double ratio = I.res0 > 0.0 ? bs / I.res0 : 0.0;
+                if (I.hist) I.hist[I.iters] = bs;
+                I.iters += 1;
+                I.ratio = ratio;
+                I.cur ^= 1;
+                if (!(bs == bs) || bs > 1e300) I.status = 3;
+                else if (tol > 0.0 && ratio < tol) I.status = 1;
+                else if (I.iters >= I.max_iter) I.status = 2;
+            }
+        }
+        if (!grid_barrier(gs, spin_limit)) return;
+    }
+}
+
 int sm_count() {
     static int n = 0;
     if (!n) {
@@ -234,6 +404,8 @@ struct gbBatchImpl {
     int variant = 0;      // register budget of the gradient/flux kernels
     int2* d_cell_items = nullptr;
     int n_cell_items = 0;
+    gb::GridSync* d_sync = nullptr;   // barrier and work counters of the persistent kernel
+    bool inject_barrier_fault = false;
     std::vector<void*> allocations;
     std::string signature;
 };
@@ -325,7 +497,65 @@ bool download_inst(Batch* b) {
            ok_(cudaStreamSynchronize(s), "batch table");
 }
 
+// One cooperative launch of the persistent kernel for `iters` iterations of
+// every active instance.  The grid is what can be resident at once (all of
+// it must be, for its barriers), capped by the work there is.
+bool launch_persistent(Batch* b, float cfl, double tol, int iters, cudaStream_t s) {
+    static int per_sm[2][2] = {{0, 0}, {0, 0}};   // [3 blocks?][transposed]
+    const size_t smem = (2 * sizeof(float4) + sizeof(uint32_t)) * kSlots * kPersistThreads;
+    const bool tr = reference_momentum();
+    const int three = b->variant == kPersistentVariant + 1;
+    void* fn = three ? (tr ? (void*)k_batch_persistent<true, 3> : (void*)k_batch_persistent<false, 3>)
+                     : (tr ? (void*)k_batch_persistent<true, 4> : (void*)k_batch_persistent<false, 4>);
+    int& n = per_sm[three][tr];
+    if (n == 0) {
+        // the blocks must all be resident at once: launch no more than fit
+        if (!ok_(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
+                 "persistent batch kernel") ||
+            !ok_(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fn, kPersistThreads, smem),
+                 "persistent batch kernel"))
+            return false;
+        if (n <= 0) { set_error("persistent batch kernel: no block fits on an SM"); return false; }
+    }
+    const int grid = std::max(1, std::min(n * sm_count(), std::max(b->n_cell_items, b->n_inst)));
+    if (!ok_(cudaMemsetAsync(b->d_sync, 0, sizeof(GridSync), s), "persistent batch kernel")) return false;
+    long long spin_limit = kBarrierSpinLimit;
+    if (b->inject_barrier_fault) {
+        // arrival counter at UINT32_MAX: the count wraps and never reaches the
+        // grid size, so no block releases the barrier; short bound
+        b->inject_barrier_fault = false;
+        spin_limit = 1 << 12;
+        if (!ok_(cudaMemsetAsync(&b->d_sync->count, 0xFF, sizeof(unsigned int), s), "persistent batch kernel"))
+            return false;
+    }
+    const int2* items = b->d_cell_items;
+    int n_items = b->n_cell_items, n_inst = b->n_inst, tile = b->tile;
+    InstDev* insts = b->d_inst;
+    const MeshTab* meshes = b->d_mesh;
+    const BcDev* bcs = b->d_bcs;
+    GridSync* gs = b->d_sync;
+    void* args[] = {(void*)&items, (void*)&n_items, (void*)&insts, (void*)&n_inst, (void*)&meshes, (void*)&tile,
+                    (void*)&bcs, (void*)&cfl, (void*)&tol, (void*)&iters, (void*)&gs, (void*)&spin_limit};
+    count_launch();
+    return ok_(cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(kPersistThreads), args, smem, s),
+               "persistent batch kernel");
+}
+
+// Whether the persistent kernel's barriers all completed (synchronises s).
+bool persistent_ok(Batch* b, cudaStream_t s) {
+    int err = 0;
+    if (!ok_(cudaMemcpyAsync(&err, &b->d_sync->error, sizeof(int), cudaMemcpyDeviceToHost, s), "batch barrier") ||
+        !ok_(cudaStreamSynchronize(s), "batch barrier"))
+        return false;
+    if (err) set_error("batch: a grid barrier wait of the persistent kernel gave up");
+    return err == 0;
+}
+
 void enqueue_iteration(Batch* b, float cfl, double tol, cudaStream_t s) {
+    if (b->variant >= kPersistentVariant) {
+        launch_persistent(b, cfl, tol, 1, s);
+        return;
+    }
     // the boundary conditions are applied by the gradient kernels (BatchGhostBcs)
     if (b->n_cell_items) {
         const int n = b->n_cell_items;
@@ -386,16 +616,21 @@ int64_t run_loop(Batch* b, float cfl, int64_t max_iter, double tol, int check_ev
         if (graph) cudaGraphDestroy(graph);
         return good;
     };
-    ok = ok && build_items(b) && capture();
+    const bool persistent = b->variant >= kPersistentVariant;
+    ok = ok && build_items(b) && (persistent || capture());
     const int tuned = b->tile;
     int64_t done = 0;
     int active = b->n_inst;
     while (ok && done < max_iter) {
         const int64_t chunk = std::min<int64_t>(check_every, max_iter - done);
-        const int per_iter = 1 + (b->n_cell_items ? 2 : 0);
-        for (int64_t i = 0; i < chunk && ok; ++i) {
-            ok = ok_(cudaGraphLaunch(exec, s), "batch graph launch");
-            count_launch(per_iter);
+        if (persistent) {
+            ok = launch_persistent(b, cfl, tol, (int)chunk, s) && persistent_ok(b, s);
+        } else {
+            const int per_iter = 1 + (b->n_cell_items ? 2 : 0);
+            for (int64_t i = 0; i < chunk && ok; ++i) {
+                ok = ok_(cudaGraphLaunch(exec, s), "batch graph launch");
+                count_launch(per_iter);
+            }
         }
         done += chunk;
         if (!ok || !download_inst(b)) { ok = false; break; }
@@ -409,7 +644,7 @@ int64_t run_loop(Batch* b, float cfl, int64_t max_iter, double tol, int check_ev
                 b->tile = t;
                 ok = size_partials(b) && upload_inst(b);
             }
-            ok = ok && build_items(b) && ok_(cudaStreamSynchronize(s), "batch items") && capture();
+            ok = ok && build_items(b) && ok_(cudaStreamSynchronize(s), "batch items") && (persistent || capture());
         }
     }
     if (exec) cudaGraphExecDestroy(exec);
@@ -507,7 +742,8 @@ gbBatch* gbBatchCreate(int n_meshes, cuMesh* const* meshes, int n_instances, con
     ok = ok && balloc(b, b->d_bcs, b->h_bcs.size(), "batch bcs") &&
          ok_(cudaMemcpyAsync(b->d_bcs, b->h_bcs.data(), b->h_bcs.size() * sizeof(BcDev), cudaMemcpyHostToDevice, s),
              "batch bcs") &&
-         balloc(b, b->d_inst, n_instances, "batch table") && size_partials(b) && build_items(b) && upload_inst(b) &&
+         balloc(b, b->d_inst, n_instances, "batch table") && balloc(b, b->d_sync, 1, "batch barrier") &&
+         size_partials(b) && build_items(b) && upload_inst(b) &&
          ok_(cudaStreamSynchronize(s), "gbBatchCreate");
     if (!ok) {
         gbBatchFree(b);
@@ -586,13 +822,20 @@ int gbBatchGetState(gbBatch* b, int inst, float* rho, float* rhou, float* rhoe) 
 int gbBatchSetTuning(gbBatch* b, int tile_cells, int schedule) {
     clear_error();
     if (!b || tile_cells < kBlock || tile_cells % kBlock || schedule < 0 || schedule >= 2 * kBatchVariants) {
-        set_error("gbBatchSetTuning: tile must be a positive multiple of 256, schedule 0..5");
+        set_error("gbBatchSetTuning: tile must be a positive multiple of 256, schedule 0..9");
         return 1;
     }
     b->tile = tile_cells;
     b->schedule = schedule & 1;
     b->variant = schedule >> 1;
     return (size_partials(b) && build_items(b) && upload_inst(b)) ? 0 : 1;
+}
+
+int gbBatchInjectBarrierFault(gbBatch* b) {
+    clear_error();
+    if (!b) { set_error("gbBatchInjectBarrierFault: null batch"); return 1; }
+    b->inject_barrier_fault = true;
+    return 0;
 }
 
 int gbBatchGetTuning(gbBatch* b, int* tile_cells, int* schedule) {
@@ -648,7 +891,8 @@ int gbBatchAutotune(gbBatch* b, gb_scalar cfl, int trial_iters, int* tile_out, i
             // one untimed iteration, then the timed trial
             if (ok) enqueue_iteration(b, cfl, 0.0, s);
             cudaEventRecord(e0, s);
-            for (int it = 0; it < iters && ok; ++it) enqueue_iteration(b, cfl, 0.0, s);
+            if (b->variant >= kPersistentVariant) ok = ok && launch_persistent(b, cfl, 0.0, iters, s);
+            else for (int it = 0; it < iters && ok; ++it) enqueue_iteration(b, cfl, 0.0, s);
             cudaEventRecord(e1, s);
             ok = ok && ok_(cudaEventSynchronize(e1), "gbBatchAutotune");
             float ms = 0.f;

@@ -227,6 +227,20 @@ struct GhostBcs {
     }
 };
 
+// How the per-cell functions read data that an iteration writes (states,
+// face states): through the read-only cache (LdNc, for kernels that never
+// write what they read in the same launch) or from L2 (LdCg, for a kernel
+// that writes those arrays itself and reads them again after a grid-wide
+// barrier, where the non-coherent read-only path could return stale lines).
+struct LdNc {
+    template <typename T>
+    __device__ __forceinline__ static T ld(const T* p) { return __ldg(p); }
+};
+struct LdCg {
+    template <typename T>
+    __device__ __forceinline__ static T ld(const T* p) { return __ldcg(p); }
+};
+
 // Per-face entry data of cell i (slot t = 0..nf-1), read straight from the
 // slot-major arrays at entry i + t N.
 struct EntriesGlobal {
@@ -269,14 +283,14 @@ __device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
 // each ghost neighbour, which carries this cell's gradient and limiter
 // (fvmScalGradLimBc / fvmVecGradLimBc, src/fvmops.cu:272-304).  nf is the
 // cell's face count; e supplies its entries.
-template <bool TRANSPOSED, typename Entries, typename Ghosts = NoGhostBcs>
+template <bool TRANSPOSED, typename Entries, typename Ghosts = NoGhostBcs, typename Ld = LdNc>
 __device__ __forceinline__ void grad_lim_cell(const MeshDev& m, EulerState q, EulerGrad g, uint32_t i, uint32_t nf,
                                               const Entries& e, const Ghosts& gh = Ghosts()) {
     float v[5];
     float4 u0;
     {
-        u0 = __ldg(&q.rhou[i]);
-        v[0] = __ldg(&q.rho[i]); v[1] = u0.x; v[2] = u0.y; v[3] = u0.z; v[4] = __ldg(&q.rhoe[i]);
+        u0 = Ld::ld(&q.rhou[i]);
+        v[0] = Ld::ld(&q.rho[i]); v[1] = u0.x; v[2] = u0.y; v[3] = u0.z; v[4] = Ld::ld(&q.rhoe[i]);
     }
     e.ready();
     float3 gs[5];
@@ -291,9 +305,9 @@ __device__ __forceinline__ void grad_lim_cell(const MeshDev& m, EulerState q, Eu
         float4 uj;
         if (!(Ghosts::kActive && j >= m.N &&
               gh.state(j, f3(__ldg(&m.cf_geo[i + t * m.N])), v[0], f3(u0), v[4], rj, uj, ej))) {
-            uj = __ldg(&q.rhou[j]);
-            rj = __ldg(&q.rho[j]);
-            ej = __ldg(&q.rhoe[j]);
+            uj = Ld::ld(&q.rhou[j]);
+            rj = Ld::ld(&q.rho[j]);
+            ej = Ld::ld(&q.rhoe[j]);
         }
         const float vj[5] = {rj, uj.x, uj.y, uj.z, ej};
 #pragma unroll
@@ -342,9 +356,9 @@ __device__ __forceinline__ void grad_lim_cell(const MeshDev& m, EulerState q, Eu
             if (Ghosts::kActive && gh.state(j, f3(__ldg(&m.cf_geo[k])), v[0], f3(u0), v[4], rj, uj, ej)) {
                 gh.store(j, rj, uj, ej);
             } else {
-                uj = __ldg(&q.rhou[j]);
-                rj = __ldg(&q.rho[j]);
-                ej = __ldg(&q.rhoe[j]);
+                uj = Ld::ld(&q.rhou[j]);
+                rj = Ld::ld(&q.rho[j]);
+                ej = Ld::ld(&q.rhoe[j]);
             }
             reconstruct<TRANSPOSED>(rj, uj, ej, gr, gu, ge, fc - f3(__ldg(&m.cell_geo[j])), rr, ru, re);
             g.rec_rho[tw] = rr;
@@ -366,6 +380,7 @@ __device__ __forceinline__ void grad_lim_cell(const MeshDev& m, EulerState q, Eu
 // dt = cfl / sum, q_new = q - F dt (into the other buffer).  Returns the
 // squared residual (F_rho^2 + |F_rhou|^2 + F_rhoE^2) V, also stored in err[i]
 // when err is not null.
+template <typename Ld = LdNc>
 __device__ __forceinline__ float flux_cell(const MeshDev& m, EulerState q, FaceRecs rec, float* __restrict__ rho_n,
                                            float4* __restrict__ rhou_n, float* __restrict__ rhoe_n,
                                            float* __restrict__ err, float cfl, uint32_t i) {
@@ -378,8 +393,8 @@ __device__ __forceinline__ float flux_cell(const MeshDev& m, EulerState q, FaceR
         const float4 gk = __ldg(&m.cf_geo[k]);
         const float3 n = f3(gk);
         const float ds = gk.w;
-        const float ra = __ldg(&rec.rho[k]), rb = __ldg(&rec.rho[t]);
-        const float4 uea = __ldg(&rec.rhou[k]), ueb = __ldg(&rec.rhou[t]);   // (rho u, rho E)
+        const float ra = Ld::ld(&rec.rho[k]), rb = Ld::ld(&rec.rho[t]);
+        const float4 uea = Ld::ld(&rec.rhou[k]), ueb = Ld::ld(&rec.rhou[t]);   // (rho u, rho E)
         const float3 ua = f3(uea), ub = f3(ueb);
         const float ea = uea.w, eb = ueb.w;
         // one reciprocal of the density per side, reused by every quotient
@@ -400,9 +415,9 @@ __device__ __forceinline__ float flux_cell(const MeshDev& m, EulerState q, FaceR
         fe -= eh * (eb - ea);
         dts += eig * ds;
     }
-    const float r0 = __ldg(&q.rho[i]);
-    const float4 u0 = __ldg(&q.rhou[i]);
-    const float e0 = __ldg(&q.rhoe[i]);
+    const float r0 = Ld::ld(&q.rho[i]);
+    const float4 u0 = Ld::ld(&q.rhou[i]);
+    const float e0 = Ld::ld(&q.rhoe[i]);
     const float dt = cfl / dts;
     rho_n[i] = r0 - fr * dt;
     rhou_n[i] = make_float4(u0.x - fu.x * dt, u0.y - fu.y * dt, u0.z - fu.z * dt, 0.f);

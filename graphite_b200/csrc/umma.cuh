@@ -72,9 +72,29 @@ __device__ __forceinline__ bool bar_try(uint64_t* bar, uint32_t parity) {
     return ok != 0;
 }
 
+// Non-blocking test of the phase with the given parity.
+__device__ __forceinline__ bool bar_test(uint64_t* bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.b32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(ok)
+        : "r"(smem_addr(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
 // Waits for the phase with the given parity to complete; gives up after
-// about `limit_cycles` SM cycles and returns false.
+// about `limit_cycles` SM cycles and returns false.  try_wait may suspend the
+// thread for a hardware-chosen time on each call, so a bound shorter than
+// that is honoured by polling with test_wait instead.
 __device__ __forceinline__ bool bar_wait(uint64_t* bar, uint32_t parity, long long limit_cycles) {
+    if (limit_cycles < (1ll << 20)) {
+        const long long t0 = clock64();
+        while (!bar_test(bar, parity))
+            if (clock64() - t0 > limit_cycles) return false;
+        return true;
+    }
     if (bar_try(bar, parity)) return true;
     const long long t0 = clock64();
     while (!bar_try(bar, parity))

@@ -98,6 +98,7 @@ struct TrainCtl {
     unsigned long long step;
     double b1t, b2t;          // beta1^(step+1), beta2^(step+1)
     int error;                // stage of a wait that gave up (0 none)
+    long long wait_cycles;    // bound of each stage's wait for its MMAs
 };
 
 // Where a tile's samples come from.
@@ -222,6 +223,7 @@ struct Cta {
     int half;                 // 0: columns 0..63 (and the per-row work), 1: columns 64..127
     uint64_t* bar;
     uint32_t phase;
+    long long wait;           // SM cycles a stage waits for its MMAs before giving up
 };
 
 // Ends a stage: publishes shared-memory writes to the tensor core, lets thread
@@ -237,7 +239,7 @@ __device__ __forceinline__ bool stage(Cta& c, Issue issue) {
         issue();
         umma::commit(c.bar);
     }
-    const bool ok = umma::bar_wait(c.bar, c.phase, kWaitCycles);
+    const bool ok = umma::bar_wait(c.bar, c.phase, c.wait);
     c.phase ^= 1u;
     const bool any_fail = __syncthreads_or(!ok);
     umma::fence_after_sync();
@@ -318,11 +320,13 @@ __device__ __forceinline__ void put_x(uint8_t* sm, int r, bool valid, const floa
     put8(sm + kSmX, kIn, r, 1, zero);
 }
 
-__device__ __forceinline__ void cta_setup(Cta& c, uint8_t* sm, const uint4* img, uint64_t* bar, uint32_t* slot) {
+__device__ __forceinline__ void cta_setup(Cta& c, uint8_t* sm, const uint4* img, uint64_t* bar, uint32_t* slot,
+                                          const TrainCtl* ctl) {
     c.sm = sm;
     c.sa = umma::smem_addr(sm);
     c.bar = bar;
     c.phase = 0;
+    c.wait = ctl->wait_cycles > 0 ? ctl->wait_cycles : kWaitCycles;
     for (int k = threadIdx.x; k < (int)(kImgBytes / 16); k += blockDim.x) reinterpret_cast<uint4*>(sm)[k] = img[k];
     if (threadIdx.x == 0) umma::bar_init(bar, 1);
     if (threadIdx.x < 32) umma::tmem_alloc(slot, kTmCols);
@@ -338,7 +342,8 @@ __device__ __forceinline__ void cta_setup(Cta& c, uint8_t* sm, const uint4* img,
 __device__ __forceinline__ void cta_teardown(Cta& c, TrainCtl* ctl, bool ok, int where) {
     if (!ok) {
         if (threadIdx.x == 0) atomicCAS(&ctl->error, 0, where);
-        // let any MMA still in flight finish (bounded) before giving TMEM back
+        // let any MMA still in flight finish (bounded by the full default,
+        // whatever the stage bound was) before giving TMEM back
         if (threadIdx.x == 0) {
             umma::commit(c.bar);
             umma::bar_wait(c.bar, c.phase, kWaitCycles);
@@ -371,7 +376,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp_train(const TrainArgs a) {
     __shared__ uint64_t bar;
     __shared__ uint32_t slot;
     Cta c;
-    cta_setup(c, sm, a.img, &bar, &slot);
+    cta_setup(c, sm, a.img, &bar, &slot, a.ctl);
     const int r = c.row;
     const bool rowwork = c.half == 0;   // the per-row work (sample, loss, thin layers) is done by half 0
     const uint32_t X = c.sa + kSmX, A1 = c.sa + kSmA1, A2 = c.sa + kSmA2, A3 = c.sa + kSmA3, DY = c.sa + kSmDY;
@@ -557,7 +562,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp_forward(const ForwardArgs a
     __shared__ uint64_t bar;
     __shared__ uint32_t slot;
     Cta c;
-    cta_setup(c, sm, a.img, &bar, &slot);
+    cta_setup(c, sm, a.img, &bar, &slot, a.ctl);
     bool ok = true;
     for (int64_t tile = blockIdx.x; tile < n_tiles && ok; tile += gridDim.x) {
         float f[8], tg[5];
@@ -702,6 +707,7 @@ struct gbWarmStartImpl {
     float* d_v = nullptr;
     uint16_t* d_img = nullptr;
     gb::TrainCtl* d_ctl = nullptr;
+    long long wait_cycles = 0;         // 0: the kernels' default bound
     float4* d_par = nullptr;
     int n_par_alloc = 0;
     uint64_t seed = 0;
@@ -764,7 +770,7 @@ bool check_ctl(WS* w, const char* what) {
 }
 
 bool reset_ctl(WS* w, cudaStream_t s) {
-    const TrainCtl h{0ull, 0.9, 0.999, 0};
+    const TrainCtl h{0ull, 0.9, 0.999, 0, w->wait_cycles};
     return ok_(cudaMemcpyAsync(w->d_ctl, &h, sizeof(h), cudaMemcpyHostToDevice, s), "warm start control");
 }
 
@@ -1143,6 +1149,13 @@ int64_t gbWarmStartTrain(gbWarmStart* w, int epochs, int tiles_per_cta, float lr
     for (void* p : {(void*)d_partials, (void*)d_lossp, (void*)d_hist})
         if (p) cudaFree(p);
     return ok ? n_steps : -1;
+}
+
+int gbWarmStartSetWaitLimit(gbWarmStart* w, long long cycles) {
+    clear_error();
+    if (!w) { set_error("gbWarmStartSetWaitLimit: null warm start"); return 1; }
+    w->wait_cycles = cycles > 0 ? cycles : 0;
+    return 0;
 }
 
 int gbWarmStartGradient(gbWarmStart* w, int64_t n, const float* x, const float* t, float* grad, double* loss) {

@@ -286,13 +286,24 @@ int gbBatchSetState(gbBatch* batch, int instance, const float* rho, const float*
 int gbBatchGetState(gbBatch* batch, int instance, float* rho, float* rhou, float* rhoe);
 
 /* Work decomposition: cells per work item (multiple of 256) and schedule =
- * order + 2 * kernel variant (schedule 0..5); order 0 runs instance by
+ * order + 2 * kernel variant (schedule 0..9); order 0 runs instance by
  * instance, 1 tile by tile across the instances of a mesh; variant 0 / 1
  * compiles the gradient and flux kernels for 4 / 5 resident 256-thread blocks
  * per SM, variant 2 runs the gradient pass in 64-thread blocks that stage
- * each cell's face entries in shared memory (flux as variant 1). */
+ * each cell's face entries in shared memory (flux as variant 1), variants 3
+ * and 4 are one persistent cooperative kernel per check_every iterations
+ * (the three phases of an iteration separated by grid-wide barriers), with 4
+ * or 3 resident 256-thread blocks per SM; a barrier wait that gives up,
+ * after a few seconds, fails the run with an error. */
 int gbBatchSetTuning(gbBatch* batch, int tile_cells, int schedule);
 int gbBatchGetTuning(gbBatch* batch, int* tile_cells, int* schedule);
+
+/* Test hook for failure detection: the next persistent launch of this batch
+ * (schedule variants 3 and 4) starts with its grid barrier in a state no block
+ * can complete, and with a short wait bound, so every block's wait gives up
+ * and the run returns an error instead of hanging; the launch after it runs
+ * normally. */
+int gbBatchInjectBarrierFault(gbBatch* batch);
 
 /* Times trial_iters iterations of every (tile, schedule) candidate from the
  * current states (restored afterwards), then the 4 fastest again over
@@ -367,6 +378,13 @@ int gbWarmStartPredict(gbWarmStart* ws, FvmField* rho, FvmField* rhou, FvmField*
  * forward: y[n][5]. */
 int gbWarmStartGradient(gbWarmStart* ws, int64_t n, const float* x, const float* t, float* grad, double* loss);
 int gbWarmStartForward(gbWarmStart* ws, int64_t n, const float* x, float* y);
+/* Bound, in SM clock cycles, on each wait of the MLP kernels for their
+ * tensor-core work (cycles <= 0: the default, about 2 s).  A wait that gives
+ * up makes the call return an error naming the stage; the kernel first lets
+ * the work in flight finish (bounded by the default) and frees its tensor
+ * memory, so later calls run normally.  Tests set a tiny bound to exercise
+ * that path without a fault. */
+int gbWarmStartSetWaitLimit(gbWarmStart* ws, long long cycles);
 
 /* Pressure force on boundary region region_id (sum of p A n over its faces,
  * n pointing out of the fluid, p of the adjacent interior cell), float64,

@@ -33,10 +33,12 @@ def _instances():
     return [(k % 2, float(rng.uniform(0.3, 0.8)), float(rng.uniform(-2, 6))) for k in range(5)]
 
 
-@pytest.mark.parametrize("tuning", [(256, 0), (512, 1), (1024, 3), (2048, 2), (512, 4), (1024, 5)])
+@pytest.mark.parametrize("tuning", [(256, 0), (512, 1), (1024, 3), (2048, 2), (512, 4), (1024, 5), (256, 6),
+                                    (512, 7), (1024, 8), (2048, 9)])
 def test_batch_equals_plain_solves(meshes, tuning):
     """Every instance of a batch follows, bit for bit, the iterates of a plain
-    solve of it, whatever the tile size and schedule."""
+    solve of it, whatever the tile size and schedule (schedules 6-9: the
+    persistent kernel)."""
     lib = capi.load()
     lib.gbSetReferenceMomentumReconstruction(1)
     cs = [EulerCase(p) for p in meshes]
@@ -63,7 +65,8 @@ def test_batch_equals_plain_solves(meshes, tuning):
         c.close()
 
 
-def test_tile_shrinks_as_instances_stop_without_changing_states(meshes):
+@pytest.mark.parametrize("schedule", [5, 7])
+def test_tile_shrinks_as_instances_stop_without_changing_states(meshes, schedule):
     """Once instances stop, the run re-tiles the remaining work into smaller
     items; every instance still ends bit for bit where a plain solve of its
     own iteration count ends, and the tuned tile is back after the run."""
@@ -73,13 +76,13 @@ def test_tile_shrinks_as_instances_stop_without_changing_states(meshes):
     inst = _instances()
     spec = [(k, airfoil_bcs(m, a)[1]) for k, m, a in inst]
     with EulerBatch(cs, spec) as b:
-        b.set_tuning(2048, 5)
+        b.set_tuning(2048, schedule)
         for i, (k, m, a) in enumerate(inst):
             b.init_uniform(i, airfoil_bcs(m, a)[0], cases.P_INF, cases.T_INF)
         done, its, rat, st = b.run(0.8, 3000, tolerance=3e-2, check_every=10)
         assert np.all(st == 1), st
         assert len(set(its.tolist())) > 1          # they stop at different iterations
-        assert b.tuning() == (2048, 5)
+        assert b.tuning() == (2048, schedule)
         got = [b.get_state(i) for i in range(len(inst))]
     for i, (k, m, a) in enumerate(inst):
         mach, bcs = airfoil_bcs(m, a)
@@ -102,7 +105,7 @@ def test_batch_instances_stop_at_their_own_tolerance(meshes):
             b.init_uniform(i, airfoil_bcs(m, a)[0], cases.P_INF, cases.T_INF)
         before = [b.get_state(i) for i in range(len(inst))]
         tile, sched = b.autotune(0.8, trial_iters=3)
-        assert tile % 256 == 0 and sched in range(6)
+        assert tile % 256 == 0 and sched in range(10)
         for i in range(len(inst)):                 # the trials' iterations are undone
             for q in range(3):
                 assert np.array_equal(b.get_state(i)[q], before[i][q])
