@@ -905,6 +905,7 @@ int64_t gbEulerRun(cuMesh* mesh, FvmField* rho, FvmField* rhou, FvmField* rhoe, 
     GhostBcTable gbt{};
     if (table_bcs) {
         gbt.n = n_regions;
+        gbt.store = inline_bcs ? 0 : 1;   // the gradient pass's ghost states are stored once, after the loop
         for (int r = 0; r <= n_regions; ++r) gbt.start[r] = mi->num.region_start[r];
         for (int r = 0; r < n_regions; ++r) gbt.type[r] = -1;
         for (int b = 0; b < n_bc; ++b) {   // a later condition on the same region replaces an earlier one
@@ -949,6 +950,12 @@ int64_t gbEulerRun(cuMesh* mesh, FvmField* rho, FvmField* rhou, FvmField* rhoe, 
     int cur = impl(rho)->cur;
     std::vector<double> hist((size_t)n_iter, 0.0);
     const int64_t done = replay_run_graphs(mi->euler_run, cur, n_iter, check_every, tolerance, hist, s, "gbEulerRun");
+    if (done > 0 && inline_bcs) {
+        // the ghost states of the last gradient pass, from the state it read
+        // (the buffer before the last update), into both value buffers
+        launch_bc_table(mi->dev, gbt, 1 - cur, s);
+        if (!launch_ok("gbEulerRun")) return -1;
+    }
     impl(rho)->cur = impl(rhou)->cur = impl(rhoe)->cur = cur;
     ei->partials_valid = true;
     if (residual_history && done > 0) memcpy(residual_history, hist.data(), (size_t)done * sizeof(double));

@@ -64,10 +64,12 @@ struct BcDev {
 // An instance's boundary conditions applied inside its gradient pass (the
 // Ghosts policy of grad_lim_cell over the batch's tables): ghost j of the
 // instance takes the condition of its region, computed by the thread of its
-// interior cell and stored into both value buffers.  On the one-layer
-// extruded meshes (about two ghosts per cell) this replaces a ghost kernel
-// that read the geometry and interior state of every ghost and wrote both
-// buffers, and the gradient pass's two gathers of each ghost state.
+// interior cell.  On the one-layer extruded meshes (about two ghosts per
+// cell) this replaces a ghost kernel that read the geometry and interior
+// state of every ghost and wrote both buffers, and the gradient pass's two
+// gathers of each ghost state.  The ghost states are not stored during the
+// iterations (nothing in them reads a ghost value that has a condition);
+// k_batch_ghosts stores those of the last gradient pass once a run ends.
 struct BatchGhostBcs {
     static constexpr bool kActive = true;
     const uint8_t* region;     // per ghost (j - N)
@@ -86,14 +88,7 @@ struct BatchGhostBcs {
         else farfield_state(nrm, r1, u1, e1, c.mach, c.p, c.t, r, ru, e);
         return true;
     }
-    __device__ __forceinline__ void store(uint32_t j, float r, float4 ru, float e) const {
-#pragma unroll
-        for (int k = 0; k < 2; ++k) {
-            rho[k][j] = r;
-            rhou[k][j] = ru;
-            rhoe[k][j] = e;
-        }
-    }
+    __device__ __forceinline__ void store(uint32_t, float, float4, float) const {}
 };
 
 __device__ __forceinline__ BatchGhostBcs batch_ghosts(const InstDev& I, const MeshTab& M, const BcDev* bcs) {
@@ -372,6 +367,36 @@ __global__ void __launch_bounds__(kPersistThreads, BLOCKS)
             }
         }
         if (!grid_barrier(gs, spin_limit)) return;
+    }
+}
+
+// After a run: every ghost of every instance that has a condition gets the
+// state its last gradient pass gave it -- the condition applied to the
+// interior state that pass read (the buffer before the last update; the
+// same slip_ghost / farfield_ghost arithmetic and normal as the pass) --
+// in both value buffers.  Block (x, instance) covers 256 of its ghosts.
+__global__ void k_batch_ghosts(const InstDev* insts, const MeshTab* __restrict__ meshes, const BcDev* __restrict__ bcs) {
+    const InstDev& I = insts[blockIdx.y];
+    const MeshTab& M = meshes[I.mesh];
+    const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= M.G || I.iters == 0) return;
+    const int b = I.bc[M.ghost_region[g]];
+    if (b < 0) return;
+    const BcDev c = bcs[b];
+    const int prev = 1 - I.cur;
+    float r, e;
+    float4 ru;
+    if (c.type == 0)
+        slip_ghost(M.m.cell_geo, M.m.face_geo, M.ghost[g], I.rho[prev], I.rhou[prev], I.rhoe[prev], r, ru, e);
+    else
+        farfield_ghost(M.m.cell_geo, M.m.face_geo, M.ghost[g], I.rho[prev], I.rhou[prev], I.rhoe[prev], c.mach, c.p,
+                       c.t, r, ru, e);
+    const uint32_t j = M.m.N + g;
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+        I.rho[k][j] = r;
+        I.rhou[k][j] = ru;
+        I.rhoe[k][j] = e;
     }
 }
 
@@ -953,7 +978,16 @@ int64_t gbBatchRun(gbBatch* b, gb_scalar cfl, int64_t max_iter, double tolerance
     reset_counters(b, max_iter, history != nullptr);
     if (!upload_inst(b)) { if (d_hist) cudaFree(d_hist); return -1; }
     const int64_t done = max_iter > 0 ? run_loop(b, cfl, max_iter, tolerance, check_every) : 0;
-    bool ok = done >= 0 && download_inst(b);
+    if (done > 0) {
+        uint32_t g_max = 0;
+        for (const MeshAccess& A : b->acc) g_max = std::max<uint32_t>(g_max, (uint32_t)A.G);
+        if (g_max > 0) {
+            k_batch_ghosts<<<dim3((g_max + kBlock - 1) / kBlock, b->n_inst), kBlock, 0, (cudaStream_t)gbGetStream()>>>(
+                b->d_inst, b->d_mesh, b->d_bcs);
+            count_launch();
+        }
+    }
+    bool ok = done >= 0 && ok_(cudaGetLastError(), "gbBatchRun") && download_inst(b);
     if (ok && history) {
         ok = ok_(cudaMemcpy(history, d_hist, (size_t)b->n_inst * max_iter * sizeof(double), cudaMemcpyDeviceToHost),
                  "gbBatchRun");

@@ -218,6 +218,7 @@ struct GhostBcs {
         return true;
     }
     __device__ __forceinline__ void store(uint32_t j, float r, float4 ru, float e) const {
+        if (!t.store) return;
 #pragma unroll
         for (int b = 0; b < 2; ++b) {
             t.rho[b][j] = r;

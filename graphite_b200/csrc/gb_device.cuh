@@ -106,10 +106,14 @@ void launch_entry_geo(const DevMesh& m, cudaStream_t s);
 // Boundary conditions the Euler gradient pass applies itself, by ghost
 // region: ghosts [start[r], start[r+1]) (absolute cell indices) get type[r]:
 // -1 none (their stored state), 0 slip, 1 far field with mach[r], p[r],
-// temp[r]; the computed ghost states are stored into both value buffers.
+// temp[r]; with store set the computed ghost states are also stored into
+// both value buffers (the replayed loop leaves them out and applies the
+// table once after its last iteration instead, k_bc_table on the buffer the
+// last gradient pass read).
 constexpr int kMaxBcRegions = 16;
 struct GhostBcTable {
     int n;
+    int store;
     uint32_t start[kMaxBcRegions + 1];
     int type[kMaxBcRegions];
     float3 mach[kMaxBcRegions];

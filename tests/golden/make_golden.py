@@ -16,7 +16,11 @@ For each case in cases.py it writes the SU2 mesh, runs the reference harness
 * prepare  - value/gradient/limiter of rho, rhou, rhoe after the boundary
              conditions and FvmEulerStepPrepare, from a seeded synthetic state;
 * solve    - residual history and final fields after a fixed number of
-             PhysicsEuler::step iterations from the uniform freestream.
+             PhysicsEuler::step iterations from the uniform freestream;
+* fvmops   - the reference's generic finite-volume operators
+             (include/fvmops.cuh:96-219) at every interior cell, from seeded
+             smooth fields, with the reference's gradients and limiters of
+             those fields (harness oracle/ref_fvmops.cu).
 """
 from __future__ import annotations
 
@@ -39,10 +43,28 @@ import cases  # noqa: E402
 import refio  # noqa: E402
 
 DRIVER = os.path.join(ROOT, "oracle", "_ref", "ref_driver")
+FVMOPS = os.path.join(ROOT, "oracle", "_ref", "ref_fvmops")
 
 METRICS = ["tet_6x3x2", "hex_6x3x2", "prism_6x3x2", "pyramid_6x3x2", "tet_12x6x2"]
 PREPARE = ["tet_6x3x2", "hex_6x3x2", "prism_6x3x2", "pyramid_6x3x2", "tet_12x6x2"]
 SOLVES = [("tet_12x6x2", 20000), ("channel", 2000), ("channel", 40000)]
+FVMOPS_MESHES = ["tet_6x3x2", "prism_6x3x2", "hex_6x3x2", "pyramid_6x3x2"]
+PHI_CONST = (0.7, -0.2, 0.4)
+
+
+def operator_fields(mesh, seed=4):
+    """Seeded smooth fields for the operator fixtures, in reference cell order
+    (cells, then ghosts at their ghost centroids): a scalar s, a vector v and
+    a vector phi."""
+    from oracle.pyoracle import OracleMesh
+
+    x = OracleMesh(mesh).get("cell_centers").reshape(-1, 3)
+    n = x.shape[0]
+    rng = np.random.default_rng(seed)
+    s = np.sin(2 * x[:, 0]) + x[:, 1] ** 2 + 0.05 * rng.standard_normal(n)
+    v = np.column_stack([np.cos(x[:, 1]), x[:, 0] * x[:, 2], 1 + 0.1 * rng.standard_normal(n)])
+    ph = np.column_stack([1 + 0.2 * x[:, 1], 0.3 * np.ones(n), -0.2 + 0.1 * x[:, 0]])
+    return s.astype(np.float32), v.astype(np.float32), ph.astype(np.float32)
 
 FLOAT_KEYS_METRICS = ["nodes", "face_areas", "face_normals", "face_centers", "cell_volumes",
                       "cell_centers", "cell_matrices"]
@@ -68,7 +90,7 @@ def main():
     a = ap.parse_args()
     os.makedirs(a.out, exist_ok=True)
     os.makedirs(a.work, exist_ok=True)
-    only = set(a.only.split(",")) if a.only else {"metrics", "prepare", "solve"}
+    only = set(a.only.split(",")) if a.only else {"metrics", "prepare", "solve", "fvmops"}
     log = open(os.path.join(a.work, "make_golden.log"), "a")
     meshes = {}
 
@@ -120,6 +142,18 @@ def main():
                                         "iterations", "wall_seconds", "event_seconds", "sizes")}
             np.savez_compressed(os.path.join(a.out, f"{name}_solve{iters}.npz"), **keep)
             print(name, iters, txt.strip().splitlines()[-1])
+    if "fvmops" in only:
+        for name in FVMOPS_MESHES:
+            m, path = su2(name)
+            sf, vf, pf = operator_fields(m)
+            fields = os.path.join(a.work, f"{name}_fvmops_fields.bin")
+            np.concatenate([sf, vf.reshape(-1), pf.reshape(-1)]).astype(np.float32).tofile(fields)
+            out = os.path.join(a.work, f"{name}_fvmops.bin")
+            run([FVMOPS, path, fields, out] + ["%.9g" % c for c in PHI_CONST], log)
+            rec = refio.read_records(out)
+            np.savez_compressed(os.path.join(a.out, f"{name}_fvmops.npz"), s=sf, v=vf, phi=pf,
+                                phi_const=np.array(PHI_CONST, np.float32), **rec)
+            print(name, "fvmops", rec["ops"].size // 35, "cells")
     log.close()
 
 
