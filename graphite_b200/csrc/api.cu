@@ -60,15 +60,18 @@ void dfree(T*& p) {
 
 // The instantiated graphs of a replayed loop (gbEulerRun / gbNSIRun), kept
 // on the mesh between calls.  `key` holds everything the captured launches
-// bake in (field identities and device buffers, CFL, boundary conditions,
-// modes); a call whose key matches replays the graphs without capturing
-// again.  The residual history of one chunk of iterations goes to `hist`
-// (capacity `cap`), the counter is reset before every chunk.
+// bake in (field identities and device buffers, CFL, tolerance, boundary
+// conditions, modes); a call whose key matches replays the graphs without
+// capturing again.  The residual history of one chunk of iterations goes to
+// `hist` (capacity `cap`); the RunCtl word stops the iterations on the
+// device once the tolerance is met (or the residual is not finite), so a
+// run ends exactly there although the host checks only every chunk.
 struct RunGraphs {
     std::vector<uint64_t> key;
     cudaGraphExec_t exec[2] = {nullptr, nullptr};
     double* hist = nullptr;
-    unsigned long long* counter = nullptr;
+    RunCtl* ctl = nullptr;            // device control word (counters, first residual, halt)
+    RunCtl* h_ctl = nullptr;          // pinned host copy
     int64_t cap = 0;
     int per_iter = 0;
     void release() {
@@ -76,9 +79,11 @@ struct RunGraphs {
             if (exec[k]) cudaGraphExecDestroy(exec[k]);
         exec[0] = exec[1] = nullptr;
         if (hist) cudaFree(hist);
-        if (counter) cudaFree(counter);
+        if (ctl) cudaFree(ctl);
+        if (h_ctl) cudaFreeHost(h_ctl);
         hist = nullptr;
-        counter = nullptr;
+        ctl = nullptr;
+        h_ctl = nullptr;
         cap = 0;
         key.clear();
     }
@@ -196,6 +201,7 @@ cuMesh* create_mesh(Topology&& topo) {
             break;
         }
         nfc[i] = (uint8_t)nf;
+        d.max_faces = std::max<int>(d.max_faces, (int)nf);
         for (uint32_t t = 0; t < nf; ++t) {
             const uint32_t k = num.start[i] + t;
             nb[entry((uint32_t)i, t)] = make_uint2(num.nb_face[k], num.nb_cell[k]);
@@ -373,21 +379,22 @@ int region_lookup(cuMesh* mesh, const char* region) {
     return -1;
 }
 
-void enqueue_slip(cuMesh* mesh, FvmField* rho, FvmField* rhou, FvmField* rhoe, int r, int cur, cudaStream_t s) {
+void enqueue_slip(cuMesh* mesh, FvmField* rho, FvmField* rhou, FvmField* rhoe, int r, int cur, cudaStream_t s,
+                  const DevMesh* dm = nullptr) {
     MeshImpl* mi = impl(mesh);
     float* pr[2] = {(float*)impl(rho)->val[0], (float*)impl(rho)->val[1]};
     float4* pu[2] = {(float4*)impl(rhou)->val[0], (float4*)impl(rhou)->val[1]};
     float* pe[2] = {(float*)impl(rhoe)->val[0], (float*)impl(rhoe)->val[1]};
-    launch_bc_slip(mi->dev, mi->num.region_start[r], mi->num.region_start[r + 1], pr, pu, pe, cur, s);
+    launch_bc_slip(dm ? *dm : mi->dev, mi->num.region_start[r], mi->num.region_start[r + 1], pr, pu, pe, cur, s);
 }
 
 void enqueue_farfield(cuMesh* mesh, FvmField* rho, FvmField* rhou, FvmField* rhoe, int r, int cur, gb_vector mach,
-                      float p, float t, cudaStream_t s) {
+                      float p, float t, cudaStream_t s, const DevMesh* dm = nullptr) {
     MeshImpl* mi = impl(mesh);
     float* pr[2] = {(float*)impl(rho)->val[0], (float*)impl(rho)->val[1]};
     float4* pu[2] = {(float4*)impl(rhou)->val[0], (float4*)impl(rhou)->val[1]};
     float* pe[2] = {(float*)impl(rhoe)->val[0], (float*)impl(rhoe)->val[1]};
-    launch_bc_farfield(mi->dev, mi->num.region_start[r], mi->num.region_start[r + 1], pr, pu, pe, cur,
+    launch_bc_farfield(dm ? *dm : mi->dev, mi->num.region_start[r], mi->num.region_start[r + 1], pr, pu, pe, cur,
                        make_float3(mach.x, mach.y, mach.z), p, t, s);
 }
 
@@ -402,11 +409,11 @@ FaceRecs recs_of(FvmField* rho, FvmField* rhou) {
 }
 
 void enqueue_flux(cuMesh* mesh, FvmField* rho, FvmField* rhou, FvmField* rhoe, FvmField* error, float cfl, int cur,
-                  cudaStream_t s) {
+                  cudaStream_t s, const DevMesh* dm = nullptr) {
     MeshImpl* mi = impl(mesh);
     const int nxt = 1 - cur;
     FieldImpl* ei = impl(error);
-    launch_flux(mi->dev, state_of(rho, rhou, rhoe, cur), recs_of(rho, rhou), (float*)impl(rho)->val[nxt],
+    launch_flux(dm ? *dm : mi->dev, state_of(rho, rhou, rhoe, cur), recs_of(rho, rhou), (float*)impl(rho)->val[nxt],
                 (float4*)impl(rhou)->val[nxt], (float*)impl(rhoe)->val[nxt], (float*)ei->val[ei->cur], ei->partials,
                 cfl, s);
 }
@@ -493,8 +500,9 @@ void key_bytes(std::vector<uint64_t>& k, const void* p, size_t n) {
 }
 
 // Makes `rg` hold graphs for `key` with a history of at least `need` entries
-// per chunk, capturing them (enqueue(k, stream, hist, counter, cap) for value
-// buffer parity k) only when the key or the capacity changed.
+// per chunk, capturing them (enqueue(k, stream, device mesh with the halt
+// word, ctl, hist, cap) for value buffer parity k) only when the key or the
+// capacity changed.
 template <class Enqueue>
 bool ensure_run_graphs(MeshImpl* mi, RunGraphs& rg, std::vector<uint64_t>& key, int64_t need, int per_iter,
                        Enqueue&& enqueue, const char* what) {
@@ -502,15 +510,21 @@ bool ensure_run_graphs(MeshImpl* mi, RunGraphs& rg, std::vector<uint64_t>& key, 
     const int64_t cap = std::max<int64_t>(need, std::max<int64_t>(256, rg.cap));
     rg.release();
     if (!mi->capture && !cuda_ok(cudaStreamCreateWithFlags(&mi->capture, cudaStreamNonBlocking), what)) return false;
-    if (!dalloc(rg.hist, (size_t)cap, what) || !dalloc(rg.counter, 1, what)) { rg.release(); return false; }
+    if (!dalloc(rg.hist, (size_t)cap, what) || !dalloc(rg.ctl, 1, what) ||
+        !cuda_ok(cudaMallocHost((void**)&rg.h_ctl, sizeof(RunCtl)), what)) {
+        rg.release();
+        return false;
+    }
     rg.cap = cap;
+    DevMesh dh = mi->dev;          // the iteration kernels of this loop stop on the halt word
+    dh.halt = &rg.ctl->halt;
     bool ok = true;
     t_counting = false;
     for (int k = 0; k < 2 && ok; ++k) {
         cudaGraph_t g = nullptr;
         ok = cuda_ok(cudaStreamBeginCapture(mi->capture, cudaStreamCaptureModeThreadLocal), "graph capture");
         if (!ok) break;
-        enqueue(k, mi->capture, rg.hist, rg.counter, (unsigned long long)cap);
+        enqueue(k, mi->capture, dh, rg.ctl, rg.hist, (unsigned long long)cap);
         ok = cuda_ok(cudaStreamEndCapture(mi->capture, &g), "graph capture") &&
              cuda_ok(cudaGraphInstantiate(&rg.exec[k], g, 0), "graph instantiate");
         if (g) cudaGraphDestroy(g);
@@ -523,45 +537,44 @@ bool ensure_run_graphs(MeshImpl* mi, RunGraphs& rg, std::vector<uint64_t>& key, 
 }
 
 // Replays the graphs from value buffer `cur` for up to n_iter iterations,
-// check_every at a time; after each chunk that chunk's residuals come back
-// to `hist` and the loop stops once one of them is below tolerance x the
-// first (tolerance > 0) or is not finite (an error).  Returns the
-// iterations run, or -1; `cur` becomes the buffer holding the last state.
-int64_t replay_run_graphs(RunGraphs& rg, int& cur, int64_t n_iter, int64_t check_every, double tolerance,
-                          std::vector<double>& hist, cudaStream_t s, const char* what) {
+// check_every at a time.  The device stops iterating once a residual is
+// below tolerance x the run's first one (tolerance > 0) or is not finite;
+// after each chunk the iterations it actually ran come back to `hist`.
+// Returns the iterations run (the last one the first below tolerance, when
+// the tolerance is met), or -1 when a residual was not finite (an error);
+// `cur` becomes the buffer holding the last state.
+int64_t replay_run_graphs(RunGraphs& rg, int& cur, int64_t n_iter, int64_t check_every, std::vector<double>& hist,
+                          cudaStream_t s, const char* what) {
+    const int cur0 = cur;
     int64_t done = 0;
-    bool ok = true;
+    bool ok = cuda_ok(cudaMemsetAsync(rg.ctl, 0, sizeof(RunCtl), s), what);
     while (ok && done < n_iter) {
         const int64_t chunk = std::min<int64_t>(check_every, n_iter - done);
-        ok = cuda_ok(cudaMemsetAsync(rg.counter, 0, sizeof(unsigned long long), s), what);
+        ok = cuda_ok(cudaMemsetAsync(&rg.ctl->it_chunk, 0, sizeof(unsigned long long), s), what);
+        int k = (int)((cur0 + done) & 1);
         for (int64_t i = 0; i < chunk && ok; ++i) {
-            ok = cuda_ok(cudaGraphLaunch(rg.exec[cur], s), "graph launch");
+            ok = cuda_ok(cudaGraphLaunch(rg.exec[k], s), "graph launch");
             count_launch(rg.per_iter);
-            cur = 1 - cur;
+            k = 1 - k;
         }
         if (!ok) break;
         ok = cuda_ok(cudaMemcpyAsync(hist.data() + done, rg.hist, (size_t)chunk * sizeof(double),
                                      cudaMemcpyDeviceToHost, s), what) &&
+             cuda_ok(cudaMemcpyAsync(rg.h_ctl, rg.ctl, sizeof(RunCtl), cudaMemcpyDeviceToHost, s), what) &&
              cuda_ok(cudaStreamSynchronize(s), what);
-        done += chunk;
         if (!ok) break;
-        bool bad = false;
-        for (int64_t i = done - chunk; i < done; ++i) bad |= !std::isfinite(hist[i]);
-        if (bad) {
+        const int64_t ran = (int64_t)std::min<unsigned long long>(rg.h_ctl->it_chunk, (unsigned long long)chunk);
+        done += ran;
+        if (rg.h_ctl->halt == 2) {
             set_error(std::string(what) + ": residual is not finite (diverged)");
             ok = false;
             break;
         }
-        if (tolerance > 0.0 && hist[0] > 0.0) {
-            bool stop = false;
-            // iterations past the first one below tolerance in this chunk already ran; all are reported
-            for (int64_t i = done - chunk; i < done && !stop; ++i) stop = hist[i] / hist[0] < tolerance;
-            if (stop) break;
-        }
+        if (rg.h_ctl->halt != 0 || ran < chunk) break;
     }
+    cur = (int)((cur0 + done) & 1);
     return ok ? done : -1;
 }
-
 }  // namespace
 
 bool mesh_access(cuMesh* mesh, MeshAccess* out) {
@@ -856,11 +869,11 @@ gb_scalar FvmFieldReduceSum(cuMesh* mesh, FvmField* var) {
     cudaStream_t s = t_stream;
     double* out = mi->dev.red + mi->dev.n_red_max;
     if (fi->partials_valid) {
-        launch_reduce_final((int)((mi->dev.N + kBlock - 1) / kBlock), fi->partials, out, nullptr, nullptr, s);
+        launch_reduce_final((int)((mi->dev.N + kBlock - 1) / kBlock), fi->partials, out, s);
     } else {
         const int nb = reduce_blocks(mi->dev.N);
         launch_reduce_partials(mi->dev.N, (const float*)fi->val[fi->cur], mi->dev.red, s);
-        launch_reduce_final(nb, mi->dev.red, out, nullptr, nullptr, s);
+        launch_reduce_final(nb, mi->dev.red, out, s);
     }
     // read back through a pinned word: a copy into pageable memory would be
     // staged by the driver
@@ -930,18 +943,20 @@ int64_t gbEulerRun(cuMesh* mesh, FvmField* rho, FvmField* rhou, FvmField* rhoe, 
     key_bytes(key, &cfl, sizeof(cfl));
     key.push_back((uint64_t)n_bc);
     if (n_bc > 0) key_bytes(key, bcs, sizeof(gbBc) * (size_t)n_bc);
+    key_bytes(key, &tolerance, sizeof(tolerance));
     // one graph per value buffer parity: BCs, gradients+limiters, flux+update, residual
-    auto enqueue = [&](int k, cudaStream_t cap, double* hist, unsigned long long* counter, unsigned long long hcap) {
-        if (table_bcs && !inline_bcs && n_bc > 0) launch_bc_table(mi->dev, gbt, k, cap);
+    auto enqueue = [&](int k, cudaStream_t cap, const DevMesh& dh, RunCtl* ctl, double* hist,
+                       unsigned long long hcap) {
+        if (table_bcs && !inline_bcs && n_bc > 0) launch_bc_table(dh, gbt, k, cap);
         for (int b = 0; b < n_bc && !table_bcs; ++b) {
-            if (bcs[b].type == 0) enqueue_slip(mesh, rho, rhou, rhoe, (int)bcs[b].region_id, k, cap);
+            if (bcs[b].type == 0) enqueue_slip(mesh, rho, rhou, rhoe, (int)bcs[b].region_id, k, cap, &dh);
             else enqueue_farfield(mesh, rho, rhou, rhoe, (int)bcs[b].region_id, k, bcs[b].mach, bcs[b].pressure,
-                                  bcs[b].temperature, cap);
+                                  bcs[b].temperature, cap, &dh);
         }
-        launch_grad_lim(mi->dev, state_of(rho, rhou, rhoe, k), grad_of(rho, rhou, rhoe, false), transposed, cap,
+        launch_grad_lim(dh, state_of(rho, rhou, rhoe, k), grad_of(rho, rhou, rhoe, false), transposed, cap,
                         inline_bcs ? &gbt : nullptr);
-        enqueue_flux(mesh, rho, rhou, rhoe, error, cfl, k, cap);
-        launch_reduce_final(nb, ei->partials, out, hist, counter, cap, hcap);
+        enqueue_flux(mesh, rho, rhou, rhoe, error, cfl, k, cap, &dh);
+        launch_reduce_final(nb, ei->partials, out, cap, ctl, hist, hcap, tolerance);
     };
     const int per_iter = (inline_bcs ? 0 : (table_bcs ? (n_bc > 0 ? 1 : 0) : n_bc)) + 3;
     if (!ensure_run_graphs(mi, mi->euler_run, key, std::min<int64_t>(check_every, n_iter), per_iter, enqueue,
@@ -949,7 +964,7 @@ int64_t gbEulerRun(cuMesh* mesh, FvmField* rho, FvmField* rhou, FvmField* rhoe, 
         return -1;
     int cur = impl(rho)->cur;
     std::vector<double> hist((size_t)n_iter, 0.0);
-    const int64_t done = replay_run_graphs(mi->euler_run, cur, n_iter, check_every, tolerance, hist, s, "gbEulerRun");
+    const int64_t done = replay_run_graphs(mi->euler_run, cur, n_iter, check_every, hist, s, "gbEulerRun");
     if (done > 0 && inline_bcs) {
         // the ghost states of the last gradient pass, from the state it read
         // (the buffer before the last update), into both value buffers
@@ -1013,21 +1028,22 @@ bool nsi_grad(cuMesh* mesh, FvmField* f) {
 }
 
 void enqueue_nsi_bc(cuMesh* mesh, FvmField* velocity, FvmField* pressure, int r, int type, int cur, gb_vector v,
-                    float pinf, cudaStream_t s) {
+                    float pinf, cudaStream_t s, const DevMesh* dm = nullptr) {
     MeshImpl* mi = impl(mesh);
     float* pp[2] = {(float*)impl(pressure)->val[0], (float*)impl(pressure)->val[1]};
     float4* pu[2] = {(float4*)impl(velocity)->val[0], (float4*)impl(velocity)->val[1]};
-    launch_nsi_bc(mi->dev, mi->num.region_start[r], mi->num.region_start[r + 1], type, pp, pu, cur,
+    launch_nsi_bc(dm ? *dm : mi->dev, mi->num.region_start[r], mi->num.region_start[r + 1], type, pp, pu, cur,
                   make_float3(v.x, v.y, v.z), pinf, s);
 }
 
 void enqueue_nsi_step(cuMesh* mesh, FvmField* velocity, FvmField* pressure, FvmField* error, float cfl, int cur,
-                      cudaStream_t s, const NsiGhostTable* ghosts = nullptr) {
+                      cudaStream_t s, const NsiGhostTable* ghosts = nullptr, const DevMesh* dm = nullptr) {
     MeshImpl* mi = impl(mesh);
+    const DevMesh& d = dm ? *dm : mi->dev;
     FieldImpl *vi = impl(velocity), *pi = impl(pressure), *ei = impl(error);
-    launch_nsi_grad(mi->dev, (const float*)pi->val[cur], (const float4*)vi->val[cur], pi->grad, vi->grad,
+    launch_nsi_grad(d, (const float*)pi->val[cur], (const float4*)vi->val[cur], pi->grad, vi->grad,
                     t_nsi.limited, s, ghosts);
-    launch_nsi_flux(mi->dev, (const float*)pi->val[cur], (const float4*)vi->val[cur], pi->grad, vi->grad,
+    launch_nsi_flux(d, (const float*)pi->val[cur], (const float4*)vi->val[cur], pi->grad, vi->grad,
                     (float*)pi->val[1 - cur], (float4*)vi->val[1 - cur], (float*)ei->val[ei->cur], ei->partials, cfl,
                     (float)t_nsi.viscosity, (float)(t_nsi.beta * t_nsi.beta), t_nsi.corrected, s);
 }
@@ -1170,13 +1186,16 @@ int64_t gbNSIRun(cuMesh* mesh, FvmField* velocity, FvmField* pressure, FvmField*
     key.push_back((uint64_t)n_bc);
     if (n_bc > 0) key_bytes(key, bcs, sizeof(gbBc) * (size_t)n_bc);
     key_bytes(key, &t_nsi, sizeof(t_nsi));
-    auto enqueue = [&](int k, cudaStream_t cap, double* hist, unsigned long long* counter, unsigned long long hcap) {
+    key_bytes(key, &tolerance, sizeof(tolerance));
+    auto enqueue = [&](int k, cudaStream_t cap, const DevMesh& dh, RunCtl* ctl, double* hist,
+                       unsigned long long hcap) {
         for (int b = 0; b < n_bc && !inline_bcs; ++b) {
             const int type = bcs[b].type == 1 ? 1 : (bcs[b].type == 2 ? 2 : 0);
-            enqueue_nsi_bc(mesh, velocity, pressure, (int)bcs[b].region_id, type, k, bcs[b].mach, bcs[b].pressure, cap);
+            enqueue_nsi_bc(mesh, velocity, pressure, (int)bcs[b].region_id, type, k, bcs[b].mach, bcs[b].pressure, cap,
+                           &dh);
         }
-        enqueue_nsi_step(mesh, velocity, pressure, error, cfl, k, cap, inline_bcs ? &gt : nullptr);
-        launch_reduce_final(nb, ei->partials, out, hist, counter, cap, hcap);
+        enqueue_nsi_step(mesh, velocity, pressure, error, cfl, k, cap, inline_bcs ? &gt : nullptr, &dh);
+        launch_reduce_final(nb, ei->partials, out, cap, ctl, hist, hcap, tolerance);
     };
     const int per_iter = (inline_bcs ? 0 : n_bc) + 3;
     if (!ensure_run_graphs(mi, mi->nsi_run, key, std::min<int64_t>(check_every, n_iter), per_iter, enqueue,
@@ -1184,7 +1203,7 @@ int64_t gbNSIRun(cuMesh* mesh, FvmField* velocity, FvmField* pressure, FvmField*
         return -1;
     int cur = impl(pressure)->cur;
     std::vector<double> hist((size_t)n_iter, 0.0);
-    const int64_t done = replay_run_graphs(mi->nsi_run, cur, n_iter, check_every, tolerance, hist, s, "gbNSIRun");
+    const int64_t done = replay_run_graphs(mi->nsi_run, cur, n_iter, check_every, hist, s, "gbNSIRun");
     impl(velocity)->cur = impl(pressure)->cur = cur;
     ei->partials_valid = true;
     if (residual_history && done > 0) memcpy(residual_history, hist.data(), (size_t)done * sizeof(double));

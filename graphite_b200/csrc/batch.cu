@@ -724,7 +724,7 @@ gbBatch* gbBatchCreate(int n_meshes, cuMesh* const* meshes, int n_instances, con
              ok_(cudaMemcpyAsync(d, reg.data(), reg.size(), cudaMemcpyHostToDevice, s), "batch regions");
         const DevMesh& D = *A.dev;
         tabs[m] = MeshTab{MeshDev{D.cell_geo, D.face_geo, D.nfc, D.nb, D.lsq, D.twin, D.cf_geo, D.nbc, D.dn, D.df,
-                                  (uint32_t)D.N, (uint32_t)D.S},
+                                  (uint32_t)D.N, (uint32_t)D.S, nullptr},
                           D.ghost, d, (uint32_t)D.G};
         b->signature += std::to_string(A.N) + "/";
     }

@@ -46,6 +46,7 @@ struct GhostBuf {
     float* rho[2];
     float4* rhou[2];
     float* rhoe[2];
+    const int* halt;
 };
 
 // euler_slip_bc, src/models/euler.cu:412-442, on the ghosts [g0, g1); written
@@ -54,7 +55,7 @@ struct GhostBuf {
 __global__ void k_bc_slip(uint32_t g0, uint32_t g1, uint32_t N, const float4* __restrict__ cell_geo,
                           const float4* __restrict__ face_geo, const uint2* __restrict__ ghost, GhostBuf b, int cur) {
     const uint32_t t = g0 + blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= g1) return;
+    if (t >= g1 || halted(b.halt)) return;
     float r, e;
     float4 ru;
     slip_ghost(cell_geo, face_geo, ghost[t - N], b.rho[cur], b.rhou[cur], b.rhoe[cur], r, ru, e);
@@ -70,7 +71,7 @@ __global__ void k_bc_farfield(uint32_t g0, uint32_t g1, uint32_t N, const float4
                               const float4* __restrict__ face_geo, const uint2* __restrict__ ghost, GhostBuf b,
                               int cur, float3 imach, float ip, float it) {
     const uint32_t t = g0 + blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= g1) return;
+    if (t >= g1 || halted(b.halt)) return;
     float r, e;
     float4 ru;
     farfield_ghost(cell_geo, face_geo, ghost[t - N], b.rho[cur], b.rhou[cur], b.rhoe[cur], imach, ip, it, r, ru, e);
@@ -86,9 +87,9 @@ __global__ void k_bc_farfield(uint32_t g0, uint32_t g1, uint32_t N, const float4
 // per-region kernels; regions of type -1 are left as they are).
 __global__ void k_bc_table(uint32_t N, uint32_t G, const float4* __restrict__ cell_geo,
                            const float4* __restrict__ face_geo, const uint2* __restrict__ ghost, GhostBcTable tb,
-                           int cur) {
+                           int cur, const int* halt) {
     const uint32_t t = N + blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= N + G) return;
+    if (t >= N + G || halted(halt)) return;
     int k = 0;
     while (k < tb.n - 1 && t >= tb.start[k + 1]) ++k;
     if (tb.type[k] < 0) return;
@@ -111,6 +112,7 @@ __global__ void k_bc_table(uint32_t N, uint32_t G, const float4* __restrict__ ce
 template <bool TRANSPOSED>
 __global__ void __launch_bounds__(kBlock, kGradBlocksPerSM) k_grad_lim(MeshDev m, EulerState q, EulerGrad g) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (halted(m.halt)) return;
     if (i < m.N) grad_lim_cell<TRANSPOSED>(m, q, g, i);
 }
 
@@ -121,30 +123,58 @@ __global__ void __launch_bounds__(kBlock, kGradBlocksPerSM) k_grad_lim(MeshDev m
 #ifndef GB_GRAD_STAGE_THREADS
 #define GB_GRAD_STAGE_THREADS 64
 #endif
-#ifndef GB_GRAD_STAGE_BLOCKS
-#define GB_GRAD_STAGE_BLOCKS 15
+// 1: the face offsets are staged too; 0: read where used (less shared memory)
+#ifndef GB_GRAD_STAGE_DF
+#define GB_GRAD_STAGE_DF 1
+#endif
+// resident blocks per SM the registers are budgeted for, by the mesh's most
+// faces per cell (shared-memory slots per thread)
+#ifndef GB_STAGE_BLOCKS_F4
+#define GB_STAGE_BLOCKS_F4 18
+#endif
+#ifndef GB_STAGE_BLOCKS_F5
+#define GB_STAGE_BLOCKS_F5 16
+#endif
+#ifndef GB_STAGE_BLOCKS_F6
+#define GB_STAGE_BLOCKS_F6 15
 #endif
 constexpr int kStageThreads = GB_GRAD_STAGE_THREADS;
+constexpr bool kStageDf = GB_GRAD_STAGE_DF != 0;
+template <int MAXF>
+constexpr int stage_blocks() {
+    return MAXF <= 4 ? GB_STAGE_BLOCKS_F4 : (MAXF == 5 ? GB_STAGE_BLOCKS_F5 : GB_STAGE_BLOCKS_F6);
+}
 
-template <bool TRANSPOSED, typename Ghosts>
-__global__ void __launch_bounds__(kStageThreads, GB_GRAD_STAGE_BLOCKS)
+// MAXF: shared-memory slots per thread, at least the mesh's most faces per cell
+template <bool TRANSPOSED, typename Ghosts, int MAXF>
+__global__ void __launch_bounds__(kStageThreads, stage_blocks<MAXF>())
     k_grad_lim_staged(MeshDev m, EulerState q, EulerGrad g, Ghosts gh) {
     constexpr int B = kStageThreads;
-    __shared__ float4 s_dn[kSlots * B], s_df[kSlots * B];
-    __shared__ uint32_t s_nbc[kSlots * B];
+    __shared__ float4 s_dn[MAXF * B], s_df[kStageDf ? MAXF * B : 1];
+    __shared__ uint32_t s_nbc[MAXF * B];
     const uint32_t tid = threadIdx.x;
     const uint32_t i = blockIdx.x * B + tid;
-    if (i >= m.N) return;
+    if (i >= m.N || halted(m.halt)) return;
     const uint32_t nf = __ldg(&m.nfc[i]);
     for (uint32_t t = 0; t < nf; ++t) {
         const uint32_t k = i + t * m.N;
         cp_async4(&s_nbc[t * B + tid], &m.nbc[k]);
         cp_async16(&s_dn[t * B + tid], &m.dn[k]);
-        cp_async16(&s_df[t * B + tid], &m.df[k]);
+        if (kStageDf) cp_async16(&s_df[t * B + tid], &m.df[k]);
     }
     asm volatile("cp.async.commit_group;\n" ::: "memory");
-    grad_lim_cell<TRANSPOSED>(m, q, g, i, nf, EntriesStaged<B>{s_nbc + tid, s_dn + tid, s_df + tid},
-                              gh);
+    if constexpr (kStageDf)
+        grad_lim_cell<TRANSPOSED>(m, q, g, i, nf, EntriesStaged<B>{s_nbc + tid, s_dn + tid, s_df + tid}, gh);
+    else
+        grad_lim_cell<TRANSPOSED>(m, q, g, i, nf, EntriesStagedDn<B>{s_nbc + tid, s_dn + tid, m.df + i, m.N}, gh);
+}
+
+template <bool TRANSPOSED, typename Ghosts>
+void launch_staged(const DevMesh& d, const MeshDev& md, EulerState q, EulerGrad g, Ghosts gh, cudaStream_t s) {
+    const unsigned gs = (unsigned)((d.N + kStageThreads - 1) / kStageThreads);
+    if (d.max_faces <= 4) k_grad_lim_staged<TRANSPOSED, Ghosts, 4><<<gs, kStageThreads, 0, s>>>(md, q, g, gh);
+    else if (d.max_faces == 5) k_grad_lim_staged<TRANSPOSED, Ghosts, 5><<<gs, kStageThreads, 0, s>>>(md, q, g, gh);
+    else k_grad_lim_staged<TRANSPOSED, Ghosts, kSlots><<<gs, kStageThreads, 0, s>>>(md, q, g, gh);
 }
 
 // Fused flux / local-time-step update / squared residual over the interior
@@ -152,6 +182,7 @@ __global__ void __launch_bounds__(kStageThreads, GB_GRAD_STAGE_BLOCKS)
 __global__ void __launch_bounds__(kBlock, kFluxBlocksPerSM)
     k_flux(MeshDev m, EulerState q, FaceRecs r, float* __restrict__ rho_n, float4* __restrict__ rhou_n,
            float* __restrict__ rhoe_n, float* __restrict__ err, double* __restrict__ partials, float cfl) {
+    if (halted(m.halt)) return;              // uniform over the grid
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     double res = 0.0;
     if (i < m.N) res = (double)flux_cell(m, q, r, rho_n, rhou_n, rhoe_n, err, cfl, i);
@@ -173,17 +204,22 @@ __global__ void k_reduce_partials(int64_t n, const float* __restrict__ v, double
     if (threadIdx.x == 0) partials[blockIdx.x] = bs;
 }
 
-__global__ void k_reduce_final(int n, const double* __restrict__ partials, double* out, double* history,
-                               unsigned long long* counter, unsigned long long history_cap) {
+__global__ void k_reduce_final(int n, const double* __restrict__ partials, double* out, RunCtl* ctl, double* history,
+                               unsigned long long history_cap, double tol) {
+    if (ctl && *(volatile int*)&ctl->halt) return;   // uniform over the block
     double s = 0.0;
     for (int i = threadIdx.x; i < n; i += blockDim.x) s += partials[i];
     const double bs = block_sum(s);
     if (threadIdx.x == 0) {
         out[0] = bs;
-        if (history) {
-            const unsigned long long it = *counter;
-            if (it < history_cap) history[it] = bs;
-            *counter = it + 1;
+        if (ctl) {
+            const unsigned long long it = ctl->it_chunk;
+            if (history && it < history_cap) history[it] = bs;
+            ctl->it_chunk = it + 1;
+            if (ctl->it_run == 0) ctl->res0 = bs;
+            ctl->it_run += 1;
+            if (!(bs == bs) || bs > 1e300) ctl->halt = 2;
+            else if (tol > 0.0 && ctl->res0 > 0.0 && bs / ctl->res0 < tol) ctl->halt = 1;
         }
     }
 }
@@ -227,7 +263,7 @@ void launch_init(int64_t n, float* rho, float4* rhou, float* rhoe, float r, floa
 void launch_bc_slip(const DevMesh& m, uint32_t g0, uint32_t g1, float* rho[2], float4* rhou[2], float* rhoe[2],
                     int cur, cudaStream_t s) {
     if (g1 <= g0) return;
-    GhostBuf b = {{rho[0], rho[1]}, {rhou[0], rhou[1]}, {rhoe[0], rhoe[1]}};
+    GhostBuf b = {{rho[0], rho[1]}, {rhou[0], rhou[1]}, {rhoe[0], rhoe[1]}, m.halt};
     k_bc_slip<<<grid(g1 - g0), kBlock, 0, s>>>(g0, g1, (uint32_t)m.N, m.cell_geo, m.face_geo, m.ghost, b, cur);
     count_launch();
 }
@@ -235,7 +271,7 @@ void launch_bc_slip(const DevMesh& m, uint32_t g0, uint32_t g1, float* rho[2], f
 void launch_bc_farfield(const DevMesh& m, uint32_t g0, uint32_t g1, float* rho[2], float4* rhou[2],
                         float* rhoe[2], int cur, float3 mach, float p, float t, cudaStream_t s) {
     if (g1 <= g0) return;
-    GhostBuf b = {{rho[0], rho[1]}, {rhou[0], rhou[1]}, {rhoe[0], rhoe[1]}};
+    GhostBuf b = {{rho[0], rho[1]}, {rhou[0], rhou[1]}, {rhoe[0], rhoe[1]}, m.halt};
     k_bc_farfield<<<grid(g1 - g0), kBlock, 0, s>>>(g0, g1, (uint32_t)m.N, m.cell_geo, m.face_geo, m.ghost, b, cur,
                                                    mach, p, t);
     count_launch();
@@ -243,13 +279,14 @@ void launch_bc_farfield(const DevMesh& m, uint32_t g0, uint32_t g1, float* rho[2
 
 void launch_bc_table(const DevMesh& m, const GhostBcTable& t, int cur, cudaStream_t s) {
     if (m.G == 0) return;
-    k_bc_table<<<grid(m.G), kBlock, 0, s>>>((uint32_t)m.N, (uint32_t)m.G, m.cell_geo, m.face_geo, m.ghost, t, cur);
+    k_bc_table<<<grid(m.G), kBlock, 0, s>>>((uint32_t)m.N, (uint32_t)m.G, m.cell_geo, m.face_geo, m.ghost, t, cur,
+                                            m.halt);
     count_launch();
 }
 
 MeshDev mesh_dev(const DevMesh& m) {
     return MeshDev{m.cell_geo, m.face_geo, m.nfc, m.nb, m.lsq, m.twin, m.cf_geo, m.nbc, m.dn, m.df,
-                   (uint32_t)m.N, (uint32_t)m.S};
+                   (uint32_t)m.N, (uint32_t)m.S, m.halt};
 }
 
 void launch_entry_geo(const DevMesh& m, cudaStream_t s) {
@@ -262,14 +299,13 @@ void launch_grad_lim(const DevMesh& m, EulerState q, EulerGrad g, bool transpose
                      const GhostBcTable* ghosts) {
     if (m.N == 0) return;
 #if GB_GRAD_STAGED
-    const unsigned gs = (unsigned)((m.N + kStageThreads - 1) / kStageThreads);
     const MeshDev md = mesh_dev(m);
     if (ghosts) {
-        if (transposed) k_grad_lim_staged<true><<<gs, kStageThreads, 0, s>>>(md, q, g, GhostBcs{*ghosts});
-        else k_grad_lim_staged<false><<<gs, kStageThreads, 0, s>>>(md, q, g, GhostBcs{*ghosts});
+        if (transposed) launch_staged<true>(m, md, q, g, GhostBcs{*ghosts}, s);
+        else launch_staged<false>(m, md, q, g, GhostBcs{*ghosts}, s);
     } else {
-        if (transposed) k_grad_lim_staged<true><<<gs, kStageThreads, 0, s>>>(md, q, g, NoGhostBcs{});
-        else k_grad_lim_staged<false><<<gs, kStageThreads, 0, s>>>(md, q, g, NoGhostBcs{});
+        if (transposed) launch_staged<true>(m, md, q, g, NoGhostBcs{}, s);
+        else launch_staged<false>(m, md, q, g, NoGhostBcs{}, s);
     }
 #else
     if (transposed) k_grad_lim<true><<<grid(m.N), kBlock, 0, s>>>(mesh_dev(m), q, g);
@@ -295,9 +331,9 @@ void launch_reduce_partials_blocks(int64_t n, const float* v, double* partials, 
     count_launch();
 }
 
-void launch_reduce_final(int n_partials, const double* partials, double* out, double* history,
-                         unsigned long long* counter, cudaStream_t s, unsigned long long history_cap) {
-    k_reduce_final<<<1, kBlock, 0, s>>>(n_partials, partials, out, history, counter, history_cap);
+void launch_reduce_final(int n_partials, const double* partials, double* out, cudaStream_t s, RunCtl* ctl,
+                         double* history, unsigned long long history_cap, double tolerance) {
+    k_reduce_final<<<1, kBlock, 0, s>>>(n_partials, partials, out, ctl, history, history_cap, tolerance);
     count_launch();
 }
 

@@ -20,7 +20,10 @@ struct MeshDev {
     const float4* df;
     uint32_t N;
     uint32_t S;
+    const int* halt;      // nonzero *halt: a stopped replayed loop's kernels return (may be null)
 };
+
+__device__ __forceinline__ bool halted(const int* halt) { return halt && *(const volatile int*)halt; }
 
 __device__ __forceinline__ float3 f3(float4 a) { return make_float3(a.x, a.y, a.z); }
 __device__ __forceinline__ float3 operator+(float3 a, float3 b) { return make_float3(a.x + b.x, a.y + b.y, a.z + b.z); }
@@ -264,6 +267,21 @@ struct EntriesStaged {
     __device__ __forceinline__ uint32_t nbc(uint32_t t) const { return s_nbc[t * B]; }
     __device__ __forceinline__ float4 dn(uint32_t t) const { return s_dn[t * B]; }
     __device__ __forceinline__ float4 df(uint32_t t) const { return s_df[t * B]; }
+    __device__ __forceinline__ void ready() const { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+};
+
+// Neighbour index and neighbour offset staged like EntriesStaged, the face
+// offset read from its slot-major array when it is used (a smaller
+// shared-memory footprint per thread).
+template <int B>
+struct EntriesStagedDn {
+    const uint32_t* s_nbc;
+    const float4* s_dn;
+    const float4* df_cell;    // &m.df[i]; slot t at t * N
+    uint32_t N;
+    __device__ __forceinline__ uint32_t nbc(uint32_t t) const { return s_nbc[t * B]; }
+    __device__ __forceinline__ float4 dn(uint32_t t) const { return s_dn[t * B]; }
+    __device__ __forceinline__ float4 df(uint32_t t) const { return __ldg(df_cell + t * N); }
     __device__ __forceinline__ void ready() const { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
 };
 

@@ -38,6 +38,7 @@ namespace gb {
 
 struct DevMesh {
     int64_t N = 0, G = 0, F = 0, S = 0;   // S = kSlots * N per-face entries
+    int max_faces = 0;                    // most faces of any interior cell (4 tet .. 6 hex)
     float4* cell_geo = nullptr;
     float4* face_geo = nullptr;
     uint8_t* nfc = nullptr;
@@ -52,6 +53,24 @@ struct DevMesh {
     // reduction scratch owned by the mesh
     double* red = nullptr;        // n_red_max partials + 1 result
     int n_red_max = 0;
+    // nonzero *halt: the iteration kernels return at once (set by
+    // k_reduce_final of a replayed loop once it has stopped); null in the
+    // mesh's own copy, set only in the copy a replayed loop is captured with
+    const int* halt = nullptr;
+};
+
+// Device control word of a replayed loop (gbEulerRun, gbNSIRun), updated by
+// k_reduce_final after each iteration's residual: that residual goes to
+// history[it_chunk] (below the history's capacity), the first of the run is
+// kept as res0, and halt becomes 1 once a residual is below tolerance x res0
+// or 2 once one is not finite; from then on the iterations left in the chunk
+// do nothing.
+struct RunCtl {
+    unsigned long long it_chunk;   // iterations run in the current chunk
+    unsigned long long it_run;     // iterations run since the loop started
+    double res0;
+    int halt;
+    int pad;
 };
 
 // Pointers of the three conserved fields as one kernel argument.
@@ -148,10 +167,11 @@ void launch_flux(const DevMesh& m, EulerState q, FaceRecs r, float* rho_n, float
 void launch_reduce_partials(int64_t n, const float* v, double* partials, cudaStream_t s);
 // stage 1 with a caller-chosen number of blocks (one partial per block)
 void launch_reduce_partials_blocks(int64_t n, const float* v, double* partials, int blocks, cudaStream_t s);
-// history (may be null): out[0] is also written to history[*counter] when
-// *counter < history_cap, and *counter is incremented
-void launch_reduce_final(int n_partials, const double* partials, double* out, double* history,
-                         unsigned long long* counter, cudaStream_t s, unsigned long long history_cap = 0);
+// Sum of the partials into out[0]; with ctl (a replayed loop) also the
+// RunCtl bookkeeping above (history may be null).
+void launch_reduce_final(int n_partials, const double* partials, double* out, cudaStream_t s,
+                         RunCtl* ctl = nullptr, double* history = nullptr, unsigned long long history_cap = 0,
+                         double tolerance = 0.0);
 
 // permute helpers for host transfers (new <-> reference order)
 void launch_gather_scalar(int64_t n, const float* src, const uint32_t* idx, float* dst, cudaStream_t s);

@@ -82,7 +82,7 @@ extern "C" int gbReduceSumNoAlloc(const float* values, uint64_t n, double* resul
     // every partial that stage 2 reads is written by stage 1 of this call,
     // so nothing left from an earlier call needs clearing
     launch_reduce_partials_blocks((int64_t)n, values, partials, blocks, s);
-    launch_reduce_final(blocks, partials, result, nullptr, nullptr, s);
+    launch_reduce_final(blocks, partials, result, s);
     const cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) {
         set_error(std::string("gbReduceSumNoAlloc: ") + cudaGetErrorString(e));

@@ -63,9 +63,9 @@ __device__ __forceinline__ void nsi_ghost_state(int type, float3 n, float pi, fl
 
 __global__ void k_nsi_bc(uint32_t g0, uint32_t g1, uint32_t N, const float4* __restrict__ cell_geo,
                          const float4* __restrict__ face_geo, const uint2* __restrict__ ghost, float* pa, float* pb,
-                         float4* ua, float4* ub, int cur, int type, float3 vinf, float pinf) {
+                         float4* ua, float4* ub, int cur, int type, float3 vinf, float pinf, const int* halt) {
     const uint32_t t = g0 + blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= g1) return;
+    if (t >= g1 || halted(halt)) return;
     const uint2 gl = ghost[t - N];
     const uint32_t c1 = gl.x;
     const float3 n = outer_normal(f3(face_geo[2 * gl.y]), f3(face_geo[2 * gl.y + 1]) - f3(cell_geo[c1]));
@@ -93,7 +93,7 @@ __global__ void __launch_bounds__(kBlock, kNsiBlocks)
     k_nsi_grad(MeshDev m, const float* __restrict__ p, const float4* __restrict__ u, float4* gp, float4* gu,
                int limited, NsiGhostTable gh) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= m.N) return;
+    if (i >= m.N || halted(m.halt)) return;
     float v[4];
     {
         const float4 ui = __ldg(&u[i]);
@@ -166,6 +166,7 @@ __global__ void __launch_bounds__(kBlock, kNsiBlocks)
     k_nsi_flux(MeshDev m, const float* __restrict__ p, const float4* __restrict__ u, const float4* __restrict__ gp,
                const float4* __restrict__ gu, float* __restrict__ p_n, float4* __restrict__ u_n,
                float* __restrict__ err, double* __restrict__ partials, NsiParams P) {
+    if (halted(m.halt)) return;              // uniform over the grid
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     double res = 0.0;
     if (i < m.N) {
@@ -302,7 +303,7 @@ void launch_nsi_bc(const DevMesh& m, uint32_t g0, uint32_t g1, int type, float* 
                    float3 vinf, float pinf, cudaStream_t s) {
     if (g1 <= g0) return;
     k_nsi_bc<<<grid_of(g1 - g0), kBlock, 0, s>>>(g0, g1, (uint32_t)m.N, m.cell_geo, m.face_geo, m.ghost, p[0], p[1],
-                                                 u[0], u[1], cur, type, vinf, pinf);
+                                                 u[0], u[1], cur, type, vinf, pinf, m.halt);
     count_launch();
 }
 

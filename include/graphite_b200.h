@@ -239,10 +239,13 @@ typedef struct gbBc {
 /* Runs n_iter iterations of the PhysicsEuler::step loop (boundary conditions
  * in the given order, prepare, step, residual sum) as a replayed CUDA graph,
  * writing the residual sum of each iteration to residual_history (host
- * array of n_iter doubles, may be NULL).  Stops early, after the iteration
- * in which residual/residual[0] < tolerance, when tolerance > 0 (checked
- * every check_every iterations; the residuals between checks are still
- * recorded).  Returns the number of iterations run, or -1 on error.
+ * array of n_iter doubles, may be NULL).  With tolerance > 0 it stops after
+ * the first iteration in which residual/residual[0] < tolerance: the device
+ * stops iterating there, although the host looks only every check_every
+ * iterations (the iterations left in that chunk do nothing).  A residual
+ * that is not finite stops it too, and the call returns -1 with "not finite"
+ * in gbGetLastError().  Returns the number of iterations run, or -1 on
+ * error.
  * The results, ghost values included, are bitwise those of the per-call
  * loop (FvmEuler*Bc, FvmEulerStepPrepare, FvmEulerStep, FvmFieldReduceSum);
  * where a region appears twice in bcs the later condition holds, and the
@@ -470,7 +473,8 @@ int FvmNSIStep(cuMesh* mesh, FvmField* velocity, FvmField* pressure, gb_scalar c
  * type 0 slip, 1 inlet / outlet (mach = inlet velocity, pressure = outlet
  * pressure), 2 no-slip wall.  The results, ghost values included, are
  * bitwise those of the per-call loop; when the ghosts number at least a
- * quarter of the cells the gradient kernel applies the conditions itself. */
+ * quarter of the cells the gradient kernel applies the conditions itself.
+ * Stops on the device at the tolerance as gbEulerRun does. */
 int64_t gbNSIRun(cuMesh* mesh, FvmField* velocity, FvmField* pressure, FvmField* error, gb_scalar cfl,
                  int64_t n_iter, const gbBc* bcs, int n_bc, double tolerance, int check_every,
                  double* residual_history);

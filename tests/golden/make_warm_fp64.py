@@ -68,10 +68,10 @@ def main():
     om = po.OracleMesh(meshgen.airfoil_extruded(120_000))
     draws = held_out_draws()[:n_cases]
     done = {}
-    if os.path.exists(OUT):
+    if os.path.exists(OUT):      # resume: keep the cases already solved
         z = np.load(OUT)
-        done = {int(k): (z["hist"][k], z["ld"][k], int(z["stop"][k])) for k in range(len(z["stop"]))
-                if z["stop"][k] != -2}
+        done = {int(k): (z["hist"][k][~np.isnan(z["hist"][k])], z["ld"][k][~np.isnan(z["ld"][k][:, 0])],
+                         int(z["stop"][k])) for k in range(len(z["stop"]))}
     results = []
     for k, (m, a) in enumerate(draws):
         if k in done:
@@ -87,7 +87,7 @@ def save(draws, results):
     n = len(results)
     L = max(len(r[0]) for r in results)
     M = max(len(r[1]) for r in results)
-    hist = np.full((n, L), np.nan)
+    hist = np.full((n, L), np.nan, np.float32)
     ld = np.full((n, M, 2), np.nan)
     for k, (h, l, _) in enumerate(results):
         hist[k, : len(h)] = h

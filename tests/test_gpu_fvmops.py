@@ -63,3 +63,42 @@ def test_operators_match_restatement(su2_paths, workdir, name):
     for f in (fs, fv, fp):
         lib.FvmFieldFree(f)
     lib.cuMeshFree(mesh)
+
+
+@pytest.mark.parametrize("name", ["tet_6x3x2", "prism_6x3x2", "hex_6x3x2", "pyramid_6x3x2"])
+def test_operators_match_reference_operators(su2_paths, workdir, name):
+    """gbFvmGradient and gbFvmApply against the reference's own operators and
+    gradients (tests/golden/<mesh>_fvmops.npz, made by oracle/ref_fvmops.cu on
+    a B200 from the same fields)."""
+    from test_oracle_golden import FVMOP_SLOTS, VECTOR_OPS
+
+    lib = capi.load()
+    z = np.load(f"{cases.__file__.rsplit('/', 1)[0]}/{name}_fvmops.npz")
+    fvm = str(workdir / f"{name}_refops.fvm")
+    capi.check(lib.cuMeshFromSu2(su2_paths(name).encode(), fvm.encode()), "cuMeshFromSu2")
+    mesh = lib.cuMeshFromFile(fvm.encode())
+    n = int(lib.cuMeshGetVarSize(mesh))
+    N = int(lib.cuMeshGetnCells(mesh))
+    assert n == len(z["s"])
+    fs, fv, fp = _field(lib, mesh, n, 1, b"s", z["s"]), _field(lib, mesh, n, 3, b"v", z["v"]), \
+        _field(lib, mesh, n, 3, b"phi", z["phi"])
+    ops = z["ops"].reshape(N, 35).astype(np.float64)
+    for f, key, k in ((fs, "s", 1), (fv, "v", 3)):
+        capi.check(lib.gbFvmGradient(mesh, f), "gbFvmGradient")
+        lib.VarAllGpuToCpu(f)
+        g, l = capi.field_gradients(f)
+        ref_g = z[f"{key}.gradient"].reshape(n, -1)[:N]
+        ref_l = z[f"{key}.limiter"].reshape(n, -1)[:N]
+        assert np.max(np.abs(g[:N] - ref_g)) <= 2e-5 * np.max(np.abs(ref_g)), key
+        assert np.max(np.abs(np.asarray(l[:N]).reshape(N, k) - ref_l)) <= 2e-4, key
+    pc = tuple(float(c) for c in z["phi_const"])
+    for op, (o, k) in FVMOP_SLOTS.items():
+        u = fv if op in VECTOR_OPS else fs
+        out = np.zeros((N, k), np.float32)
+        capi.check(lib.gbFvmApply(mesh, op, u, fp, capi.vec(pc), out.ctypes.data), f"gbFvmApply {op}")
+        ref = ops[:, o:o + k]
+        scale = max(np.max(np.abs(ref)), 1e-12)
+        assert np.max(np.abs(out - ref)) <= 1e-4 * scale, (op, np.max(np.abs(out - ref)) / scale)
+    for f in (fs, fv, fp):
+        lib.FvmFieldFree(f)
+    lib.cuMeshFree(mesh)

@@ -100,3 +100,39 @@ def test_channel_2000_iterations_match_reference():
         o = s.get(ok)[:N]
         d = np.abs(o - r) / np.max(np.abs(r))
         assert d.max() < 1e-3 and d.mean() < 5e-5, (key, d.max(), d.mean())
+
+
+# (offset, width) of each operator in the reference harness's 35 outputs per
+# cell (oracle/ref_fvmops.cu), by the operator ids of gbFvmApply
+FVMOP_SLOTS = {0: (0, 1), 1: (1, 3), 2: (4, 3), 3: (7, 9), 4: (16, 3), 5: (19, 9), 6: (28, 1), 7: (29, 1),
+               8: (30, 1), 9: (31, 1), 10: (32, 3)}
+VECTOR_OPS = (3, 5, 6, 10)
+
+
+@pytest.mark.parametrize("name", ["tet_6x3x2", "prism_6x3x2", "hex_6x3x2", "pyramid_6x3x2"])
+def test_operator_restatement_matches_reference_operators(name):
+    """oracle/fvmops_oracle.py against the reference's own inline fvmOp
+    functions (include/fvmops.cuh:96-219) evaluated by oracle/ref_fvmops.cu
+    on the B200 (float32, fast math), given the reference's own gradients
+    and limiters; and the restated gradient + limiter against the
+    reference's ScalarVar/VectorVarComputeGradient and -Limiters."""
+    from oracle.fvmops_oracle import OpMesh
+
+    z = np.load(f"{cases.__file__.rsplit('/', 1)[0]}/{name}_fvmops.npz")
+    om = OpMesh(OracleMesh(cases.MESHES[name]()))
+    N, n = om.N, len(z["s"])
+    ops = z["ops"].reshape(N, 35).astype(np.float64)
+    s, v = z["s"].astype(np.float64), z["v"].astype(np.float64)
+    sg = z["s.gradient"].reshape(n, 3)[:N].astype(np.float64)
+    sl = z["s.limiter"][:N].astype(np.float64)
+    vg = z["v.gradient"].reshape(n, 3, 3)[:N].astype(np.float64)     # tensor columns = component gradients
+    vl = z["v.limiter"].reshape(n, 3)[:N].astype(np.float64)
+    g, l = om.gradient(s)
+    assert rel_max(g[:, 0], sg) < 2e-5 and np.max(np.abs(l[:, 0] - sl)) < 2e-5
+    g, l = om.gradient(v)
+    assert rel_max(g, vg) < 2e-5 and np.max(np.abs(l - vl)) < 2e-5
+    for op, (o, k) in FVMOP_SLOTS.items():
+        u = v if op in VECTOR_OPS else s
+        got = om.apply(op, u, grad=sg[:, None, :], lim=sl[:, None], phi=z["phi"].astype(np.float64),
+                       phi_c=z["phi_const"].astype(np.float64)).reshape(N, k)
+        assert rel_max(got, ops[:, o:o + k]) < 1e-4, op
