@@ -53,6 +53,8 @@ struct MeshTab {
     const uint2* ghost;
     const uint8_t* ghost_region;
     uint32_t G;
+    int n_regions;
+    uint32_t region_start[kMaxRegions + 1];   // ghost cells of region r: [start[r], start[r+1])
 };
 
 struct BcDev {
@@ -70,30 +72,54 @@ struct BcDev {
 // gathers of each ghost state.  The ghost states are not stored during the
 // iterations (nothing in them reads a ghost value that has a condition);
 // k_batch_ghosts stores those of the last gradient pass once a run ends.
+// An instance's conditions by region, as a block holds them in shared memory
+// while it works on the instance: ghost cells [start[r], start[r+1]) take
+// condition r (type -1: none, the stored state).
+struct BatchBcShared {
+    uint32_t start[kMaxRegions + 1];
+    int n;
+    int type[kMaxRegions];
+    float3 mach[kMaxRegions];
+    float p[kMaxRegions], t[kMaxRegions];
+};
+
 struct BatchGhostBcs {
     static constexpr bool kActive = true;
-    const uint8_t* region;     // per ghost (j - N)
-    const int* bc;             // per region: index into bcs, -1 none
-    const BcDev* bcs;
-    uint32_t N;
-    float* rho[2];
-    float4* rhou[2];
-    float* rhoe[2];
+    const BatchBcShared* tb;   // shared memory
     __device__ __forceinline__ bool state(uint32_t j, float3 nrm, float r1, float3 u1, float e1, float& r, float4& ru,
                                           float& e) const {
-        const int b = bc[region[j - N]];
-        if (b < 0) return false;
-        const BcDev c = bcs[b];
-        if (c.type == 0) slip_state(nrm, r1, u1, e1, r, ru, e);
-        else farfield_state(nrm, r1, u1, e1, c.mach, c.p, c.t, r, ru, e);
+        int k = 0;
+        while (k < tb->n - 1 && j >= tb->start[k + 1]) ++k;
+        const int type = tb->type[k];
+        if (type < 0) return false;
+        if (type == 0) slip_state(nrm, r1, u1, e1, r, ru, e);
+        else farfield_state(nrm, r1, u1, e1, tb->mach[k], tb->p[k], tb->t[k], r, ru, e);
         return true;
     }
     __device__ __forceinline__ void store(uint32_t, float, float4, float) const {}
 };
 
-__device__ __forceinline__ BatchGhostBcs batch_ghosts(const InstDev& I, const MeshTab& M, const BcDev* bcs) {
-    return BatchGhostBcs{M.ghost_region, I.bc, bcs, M.m.N, {I.rho[0], I.rho[1]}, {I.rhou[0], I.rhou[1]},
-                         {I.rhoe[0], I.rhoe[1]}};
+// The block's copy of instance I's conditions.  Every thread of the block
+// calls it (it ends with a barrier); blockDim.x > kMaxRegions.
+__device__ __forceinline__ BatchGhostBcs batch_ghosts(BatchBcShared& sh, const InstDev& I, const MeshTab& M,
+                                                      const BcDev* bcs) {
+    const int r = threadIdx.x;
+    if (r == 0) sh.n = M.n_regions;
+    if (r <= M.n_regions) sh.start[r] = M.region_start[r];
+    if (r < M.n_regions) {
+        const int b = I.bc[r];
+        if (b >= 0) {
+            const BcDev c = bcs[b];
+            sh.type[r] = c.type;
+            sh.mach[r] = c.mach;
+            sh.p[r] = c.p;
+            sh.t[r] = c.t;
+        } else {
+            sh.type[r] = -1;
+        }
+    }
+    __syncthreads();
+    return BatchGhostBcs{&sh};
 }
 
 // Four forms of the batched iteration: variant 0 and 1 are two register
@@ -115,12 +141,13 @@ template <bool TRANSPOSED, int BLOCKS>
 __global__ void __launch_bounds__(kBlock, BLOCKS)
     k_batch_grad(const int2* __restrict__ items, const InstDev* insts, const MeshTab* __restrict__ meshes, int tile,
                  const BcDev* __restrict__ bcs) {
+    __shared__ BatchBcShared s_bc;
     const int2 w = items[blockIdx.x];
     const InstDev& I = insts[w.x];
     if (I.status) return;
     const MeshTab& M = meshes[I.mesh];
     const MeshDev m = M.m;
-    const BatchGhostBcs gh = batch_ghosts(I, M, bcs);
+    const BatchGhostBcs gh = batch_ghosts(s_bc, I, M, bcs);
     const int cur = I.cur;
     const EulerState q{I.rho[cur], I.rhou[cur], I.rhoe[cur]};
     const EulerGrad g{nullptr, nullptr, nullptr, I.rec_rho, I.rec_rhou};
@@ -130,39 +157,40 @@ __global__ void __launch_bounds__(kBlock, BLOCKS)
         grad_lim_cell<TRANSPOSED>(m, q, g, i, __ldg(&m.nfc[i]), EntriesGlobal{m, i}, gh);
 }
 
+// One cell per thread: work item k's tile is split over tile / 64 blocks
+// (block b takes sub-tile b % subs of item b / subs), as the single-mesh
+// staged kernel covers a mesh, so that every cell's loads are in flight at
+// once instead of a thread taking its item's cells one after another.
 template <bool TRANSPOSED>
 __global__ void __launch_bounds__(kStagedThreads, kStagedBlocks)
     k_batch_grad_staged(const int2* __restrict__ items, const InstDev* insts, const MeshTab* __restrict__ meshes,
-                        int tile, const BcDev* __restrict__ bcs) {
+                        int tile, const BcDev* __restrict__ bcs, int subs) {
     constexpr int B = kStagedThreads;
     __shared__ float4 s_dn[kSlots * B], s_df[kSlots * B];
     __shared__ uint32_t s_nbc[kSlots * B];
-    const int2 w = items[blockIdx.x];
+    __shared__ BatchBcShared s_bc;
+    const int2 w = items[blockIdx.x / subs];
     const InstDev& I = insts[w.x];
-    if (I.status) return;
+    if (I.status) return;                      // uniform over the block
     const MeshTab& M = meshes[I.mesh];
     const MeshDev m = M.m;
-    const BatchGhostBcs gh = batch_ghosts(I, M, bcs);
+    const uint32_t tid = threadIdx.x;
+    const uint32_t i = (uint32_t)w.y * tile + (blockIdx.x % subs) * B + tid;
+    const uint32_t c1 = min(m.N, (uint32_t)w.y * tile + (uint32_t)tile);
+    const BatchGhostBcs gh = batch_ghosts(s_bc, I, M, bcs);   // before any thread leaves
+    if (i >= c1) return;
     const int cur = I.cur;
     const EulerState q{I.rho[cur], I.rhou[cur], I.rhoe[cur]};
     const EulerGrad g{nullptr, nullptr, nullptr, I.rec_rho, I.rec_rhou};
-    const uint32_t c0 = (uint32_t)w.y * tile;
-    const uint32_t c1 = min(m.N, c0 + (uint32_t)tile);
-    const uint32_t tid = threadIdx.x;
-    // the slots are this thread's own; the previous cell's reads of them have
-    // completed before its results were stored
-    for (uint32_t i = c0 + tid; i < c1; i += B) {
-        const uint32_t nf = __ldg(&m.nfc[i]);
-        for (uint32_t t = 0; t < nf; ++t) {
-            const uint32_t k = i + t * m.N;
-            cp_async4(&s_nbc[t * B + tid], &m.nbc[k]);
-            cp_async16(&s_dn[t * B + tid], &m.dn[k]);
-            cp_async16(&s_df[t * B + tid], &m.df[k]);
-            }
-        asm volatile("cp.async.commit_group;\n" ::: "memory");
-        grad_lim_cell<TRANSPOSED>(m, q, g, i, nf, EntriesStaged<B>{s_nbc + tid, s_dn + tid, s_df + tid},
-                                  gh);
+    const uint32_t nf = __ldg(&m.nfc[i]);
+    for (uint32_t t = 0; t < nf; ++t) {
+        const uint32_t k = i + t * m.N;
+        cp_async4(&s_nbc[t * B + tid], &m.nbc[k]);
+        cp_async16(&s_dn[t * B + tid], &m.dn[k]);
+        cp_async16(&s_df[t * B + tid], &m.df[k]);
     }
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+    grad_lim_cell<TRANSPOSED>(m, q, g, i, nf, EntriesStaged<B>{s_nbc + tid, s_dn + tid, s_df + tid}, gh);
 }
 
 template <int BLOCKS>
@@ -293,6 +321,7 @@ __global__ void __launch_bounds__(kPersistThreads, BLOCKS)
     float4* s_dn = s_stage;
     float4* s_df = s_stage + kSlots * B;
     uint32_t* s_nbc = reinterpret_cast<uint32_t*>(s_stage + 2 * kSlots * B);
+    __shared__ BatchBcShared s_bc;
     const uint32_t tid = threadIdx.x;
     for (int it = 0; it < iters; ++it) {
         // phase 0: gradients, limiters, face states (boundary conditions applied inside)
@@ -304,7 +333,7 @@ __global__ void __launch_bounds__(kPersistThreads, BLOCKS)
             if (__ldcg(&I.status)) continue;           // uniform over the block
             const MeshTab& M = meshes[I.mesh];
             const MeshDev m = M.m;
-            const BatchGhostBcs gh = batch_ghosts(I, M, bcs);
+            const BatchGhostBcs gh = batch_ghosts(s_bc, I, M, bcs);   // grab_item's barrier: the last item is done with it
             const int cur = __ldcg(&I.cur);
             const EulerState q{I.rho[cur], I.rhou[cur], I.rhoe[cur]};
             const EulerGrad g{nullptr, nullptr, nullptr, I.rec_rho, I.rec_rhou};
@@ -594,8 +623,9 @@ void enqueue_iteration(Batch* b, float cfl, double tol, cudaStream_t s) {
             else k_batch_grad<false, kBatchGradBlocks[1]><<<n, kBlock, 0, s>>>(b->d_cell_items, b->d_inst, b->d_mesh, b->tile, b->d_bcs);
             k_batch_flux<kBatchFluxBlocks[1]><<<n, kBlock, 0, s>>>(b->d_cell_items, b->d_inst, b->d_mesh, b->tile, cfl);
         } else {
-            if (tr) k_batch_grad_staged<true><<<n, kStagedThreads, 0, s>>>(b->d_cell_items, b->d_inst, b->d_mesh, b->tile, b->d_bcs);
-            else k_batch_grad_staged<false><<<n, kStagedThreads, 0, s>>>(b->d_cell_items, b->d_inst, b->d_mesh, b->tile, b->d_bcs);
+            const int subs = b->tile / kStagedThreads;
+            if (tr) k_batch_grad_staged<true><<<n * subs, kStagedThreads, 0, s>>>(b->d_cell_items, b->d_inst, b->d_mesh, b->tile, b->d_bcs, subs);
+            else k_batch_grad_staged<false><<<n * subs, kStagedThreads, 0, s>>>(b->d_cell_items, b->d_inst, b->d_mesh, b->tile, b->d_bcs, subs);
             k_batch_flux<kBatchFluxBlocks[1]><<<n, kBlock, 0, s>>>(b->d_cell_items, b->d_inst, b->d_mesh, b->tile, cfl);
         }
     }
@@ -725,7 +755,8 @@ gbBatch* gbBatchCreate(int n_meshes, cuMesh* const* meshes, int n_instances, con
         const DevMesh& D = *A.dev;
         tabs[m] = MeshTab{MeshDev{D.cell_geo, D.face_geo, D.nfc, D.nb, D.lsq, D.twin, D.cf_geo, D.nbc, D.dn, D.df,
                                   (uint32_t)D.N, (uint32_t)D.S, nullptr},
-                          D.ghost, d, (uint32_t)D.G};
+                          D.ghost, d, (uint32_t)D.G, A.n_regions, {}};
+        for (int r = 0; r <= A.n_regions; ++r) tabs[m].region_start[r] = A.region_start[r];
         b->signature += std::to_string(A.N) + "/";
     }
     ok = ok && balloc(b, b->d_mesh, n_meshes, "batch meshes") &&
