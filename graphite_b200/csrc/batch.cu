@@ -157,40 +157,39 @@ __global__ void __launch_bounds__(kBlock, BLOCKS)
         grad_lim_cell<TRANSPOSED>(m, q, g, i, __ldg(&m.nfc[i]), EntriesGlobal{m, i}, gh);
 }
 
-// One cell per thread: work item k's tile is split over tile / 64 blocks
-// (block b takes sub-tile b % subs of item b / subs), as the single-mesh
-// staged kernel covers a mesh, so that every cell's loads are in flight at
-// once instead of a thread taking its item's cells one after another.
 template <bool TRANSPOSED>
 __global__ void __launch_bounds__(kStagedThreads, kStagedBlocks)
     k_batch_grad_staged(const int2* __restrict__ items, const InstDev* insts, const MeshTab* __restrict__ meshes,
-                        int tile, const BcDev* __restrict__ bcs, int subs) {
+                        int tile, const BcDev* __restrict__ bcs) {
     constexpr int B = kStagedThreads;
     __shared__ float4 s_dn[kSlots * B], s_df[kSlots * B];
     __shared__ uint32_t s_nbc[kSlots * B];
     __shared__ BatchBcShared s_bc;
-    const int2 w = items[blockIdx.x / subs];
+    const int2 w = items[blockIdx.x];
     const InstDev& I = insts[w.x];
     if (I.status) return;                      // uniform over the block
     const MeshTab& M = meshes[I.mesh];
     const MeshDev m = M.m;
-    const uint32_t tid = threadIdx.x;
-    const uint32_t i = (uint32_t)w.y * tile + (blockIdx.x % subs) * B + tid;
-    const uint32_t c1 = min(m.N, (uint32_t)w.y * tile + (uint32_t)tile);
-    const BatchGhostBcs gh = batch_ghosts(s_bc, I, M, bcs);   // before any thread leaves
-    if (i >= c1) return;
+    const BatchGhostBcs gh = batch_ghosts(s_bc, I, M, bcs);
     const int cur = I.cur;
     const EulerState q{I.rho[cur], I.rhou[cur], I.rhoe[cur]};
     const EulerGrad g{nullptr, nullptr, nullptr, I.rec_rho, I.rec_rhou};
-    const uint32_t nf = __ldg(&m.nfc[i]);
-    for (uint32_t t = 0; t < nf; ++t) {
-        const uint32_t k = i + t * m.N;
-        cp_async4(&s_nbc[t * B + tid], &m.nbc[k]);
-        cp_async16(&s_dn[t * B + tid], &m.dn[k]);
-        cp_async16(&s_df[t * B + tid], &m.df[k]);
+    const uint32_t c0 = (uint32_t)w.y * tile;
+    const uint32_t c1 = min(m.N, c0 + (uint32_t)tile);
+    const uint32_t tid = threadIdx.x;
+    // the slots are this thread's own; the previous cell's reads of them have
+    // completed before its results were stored
+    for (uint32_t i = c0 + tid; i < c1; i += B) {
+        const uint32_t nf = __ldg(&m.nfc[i]);
+        for (uint32_t t = 0; t < nf; ++t) {
+            const uint32_t k = i + t * m.N;
+            cp_async4(&s_nbc[t * B + tid], &m.nbc[k]);
+            cp_async16(&s_dn[t * B + tid], &m.dn[k]);
+            cp_async16(&s_df[t * B + tid], &m.df[k]);
+        }
+        asm volatile("cp.async.commit_group;\n" ::: "memory");
+        grad_lim_cell<TRANSPOSED>(m, q, g, i, nf, EntriesStaged<B>{s_nbc + tid, s_dn + tid, s_df + tid}, gh);
     }
-    asm volatile("cp.async.commit_group;\n" ::: "memory");
-    grad_lim_cell<TRANSPOSED>(m, q, g, i, nf, EntriesStaged<B>{s_nbc + tid, s_dn + tid, s_df + tid}, gh);
 }
 
 template <int BLOCKS>
@@ -623,9 +622,8 @@ void enqueue_iteration(Batch* b, float cfl, double tol, cudaStream_t s) {
             else k_batch_grad<false, kBatchGradBlocks[1]><<<n, kBlock, 0, s>>>(b->d_cell_items, b->d_inst, b->d_mesh, b->tile, b->d_bcs);
             k_batch_flux<kBatchFluxBlocks[1]><<<n, kBlock, 0, s>>>(b->d_cell_items, b->d_inst, b->d_mesh, b->tile, cfl);
         } else {
-            const int subs = b->tile / kStagedThreads;
-            if (tr) k_batch_grad_staged<true><<<n * subs, kStagedThreads, 0, s>>>(b->d_cell_items, b->d_inst, b->d_mesh, b->tile, b->d_bcs, subs);
-            else k_batch_grad_staged<false><<<n * subs, kStagedThreads, 0, s>>>(b->d_cell_items, b->d_inst, b->d_mesh, b->tile, b->d_bcs, subs);
+            if (tr) k_batch_grad_staged<true><<<n, kStagedThreads, 0, s>>>(b->d_cell_items, b->d_inst, b->d_mesh, b->tile, b->d_bcs);
+            else k_batch_grad_staged<false><<<n, kStagedThreads, 0, s>>>(b->d_cell_items, b->d_inst, b->d_mesh, b->tile, b->d_bcs);
             k_batch_flux<kBatchFluxBlocks[1]><<<n, kBlock, 0, s>>>(b->d_cell_items, b->d_inst, b->d_mesh, b->tile, cfl);
         }
     }

@@ -2,10 +2,9 @@
 // callers that cannot allocate device memory.
 //
 // Some callers cannot call cudaMalloc at the point where they need a
-// reduction: code that is recording a CUDA graph (cudaMalloc is not a
-// capturable operation), hosts that hand out all device memory from their own
-// pool and forbid other allocations, and plugins that must keep their device
-// footprint fixed after setup.  The mesh/field entry points allocate their
+// reduction: hosts that hand out all device memory from their own pool and
+// forbid other allocations, and plugins that must keep their device footprint
+// fixed after setup.  The mesh/field entry points allocate their
 // scratch (reduction partials, gradients) on first use; this entry point
 // allocates nothing.  Its scratch -- one float64 partial sum per block of
 // 2048 inputs -- lives in the file-scope array below, which every GPU that
@@ -29,7 +28,10 @@ static __device__ __align__(256) double g_noalloc_partials[kNoAllocPartials];
 
 // Device address of g_noalloc_partials, resolved once per device.  In host
 // code the array's name is only a host-side stand-in for the symbol, so the
-// kernels are given this address.
+// kernels are given this address.  The cached address belongs to the
+// device's current context: after cudaDeviceReset the module may load at
+// another address, so a caller that resets a device must not use this entry
+// point on it again in the same process.
 std::mutex g_mu;
 double* g_ptr[kMaxDevices] = {nullptr};
 
@@ -58,6 +60,18 @@ bool scratch_for_current_device(double** out) {
     return true;
 }
 
+// Whether p is device (or managed) memory this context can write: a host
+// pointer given here would be written through by the kernel.
+bool device_pointer(const void* p) {
+    cudaPointerAttributes a{};
+    const cudaError_t e = cudaPointerGetAttributes(&a, p);
+    if (e != cudaSuccess) {
+        cudaGetLastError();   // the error is not sticky; clear it so later calls do not see it
+        return false;
+    }
+    return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+
 }  // namespace
 }  // namespace gb
 
@@ -65,8 +79,8 @@ using namespace gb;
 
 extern "C" int gbReduceSumNoAlloc(const float* values, uint64_t n, double* result, void* stream) {
     clear_error();
-    if (!values || !result) {
-        set_error("gbReduceSumNoAlloc: values and result must be device pointers");
+    if (!values || !result || !device_pointer(values) || !device_pointer(result)) {
+        set_error("gbReduceSumNoAlloc: values and result must be device (or managed) memory");
         return 1;
     }
     if (n > (uint64_t)kNoAllocMaxItems) {

@@ -484,18 +484,20 @@ int gbNSIWallForce(cuMesh* mesh, FvmField* velocity, FvmField* pressure, unsigne
 
 /* Sum of n float values in device memory into *result (one double in device
  * memory), accumulated in float64 in a fixed order: the reduction behind
- * FvmFieldReduceSum, for callers that cannot allocate device memory -- code
- * recording a CUDA graph (cudaMalloc cannot be captured), hosts that hand out
- * all device memory from their own pool, plugins whose device footprint must
- * not grow after setup.  It allocates nothing: its scratch is a static array
- * of 4096 partial sums (32 KiB per GPU, held by every GPU that loads the
- * library until exit), so n is limited to 4096 * 2048 = 8,388,608; larger n
- * is rejected with an error.  The first call on each device looks the array
- * up (cudaGetSymbolAddress) and should come before any stream capture.  All
- * calls share the array: calls that overlap on the GPU (other streams, other
- * threads) race and must be ordered by the caller.  Asynchronous on `stream`
- * (a cudaStream_t; NULL = legacy default stream).  Returns 0, or nonzero with
- * gbGetLastError set.  No counterpart in the reference. */
+ * FvmFieldReduceSum, for callers that cannot allocate device memory -- hosts
+ * that hand out all device memory from their own pool, plugins whose device
+ * footprint must not grow after setup.  It allocates nothing: its scratch is
+ * a static array of 4096 partial sums (32 KiB per GPU, held by every GPU that
+ * loads the library until exit), so n is limited to 4096 * 2048 = 8,388,608;
+ * larger n is rejected with an error.  values and result must be device (or
+ * managed) memory; other pointers are rejected.  The first call on each
+ * device looks the array up (cudaGetSymbolAddress) and should come before
+ * any stream capture; the address it keeps does not survive a
+ * cudaDeviceReset of that device.  All calls share the array: calls that
+ * overlap on the GPU (other streams, other threads) race and must be ordered
+ * by the caller.  Asynchronous on `stream` (a cudaStream_t; NULL = legacy
+ * default stream).  Returns 0, or nonzero with gbGetLastError set.  No
+ * counterpart in the reference. */
 int gbReduceSumNoAlloc(const float* values, uint64_t n, double* result, void* stream);
 
 #ifdef __cplusplus

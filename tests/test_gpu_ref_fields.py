@@ -16,11 +16,12 @@ as those.  It also agrees with
 the float64 oracle at least as closely as the reference's float32 runs do.
 
 Measured on the B200 (relative L2, the largest over rho, rho u, rho E):
-channel, 2,000 iterations -- twelve reference runs 2.3e-6..5.4e-5 apart,
-this library 8.1e-6..5.7e-5 from them and 9.3e-6 from the float64 oracle
-(the reference's float32 runs 1.6e-5..5.7e-5 from it); airfoil (4,608
-prisms), 30,000 iterations -- four reference runs 1.6e-4..4.0e-4 apart, this
-library 9.5e-5..2.4e-4 from them."""
+channel, 2,000 iterations -- twelve reference runs 3.1e-6..5.9e-5 apart,
+this library 6.4e-6..6.1e-5 from them and 9.3e-6 from the float64 oracle
+(the reference's float32 runs 5.6e-5..5.9e-5 from it); airfoil (4,608
+prisms), 30,000 iterations -- six reference runs 9.2e-5..3.8e-4 apart, this
+library 1.2e-4..3.4e-4 from them and 2.7e-4 from the float64 oracle (the
+reference's float32 runs 3.0e-4..3.9e-4)."""
 import math
 import os
 import subprocess

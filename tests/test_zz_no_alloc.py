@@ -1,7 +1,7 @@
 """gbReduceSumNoAlloc, the reduction entry point that allocates no device
-memory (for callers that cannot call cudaMalloc: code recording a CUDA graph,
-hosts that own all device memory through their own pool, plugins whose device
-footprint is fixed after setup).
+memory (for callers that cannot call cudaMalloc: hosts that own all device
+memory through their own pool, plugins whose device footprint is fixed after
+setup).
 
 It is checked through the C ABI against the entry point it mirrors,
 FvmFieldReduceSum, on the same values, on two calls in a row (the scratch
@@ -79,3 +79,11 @@ def test_no_alloc_limits_and_reuse():
     rc = lib.gbReduceSumNoAlloc(ctypes.c_void_p(big.data_ptr()), 8_388_609, ctypes.c_void_p(out.data_ptr()),
                                 ctypes.c_void_p(stream))
     assert rc != 0 and "exceed the maximum" in capi.last_error()
+    # a host pointer for the result is rejected before any launch
+    host = np.zeros(1, np.float64)
+    rc = lib.gbReduceSumNoAlloc(ctypes.c_void_p(small.data_ptr()), small.numel(),
+                                ctypes.c_void_p(host.ctypes.data), ctypes.c_void_p(stream))
+    assert rc != 0 and "device" in capi.last_error() and host[0] == 0.0
+    _reduce_no_alloc(lib, small, small.numel(), out, stream)     # and the next call works
+    torch.cuda.synchronize()
+    assert out.item() == 3000.0
