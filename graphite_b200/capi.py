@@ -141,6 +141,7 @@ _PROTOS = {
     "gbWarmStartForward": (C.c_int, [C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p]),
     "gbWarmStartSetWaitLimit": (C.c_int, [C.c_void_p, C.c_longlong]),
     "gbBatchInjectBarrierFault": (C.c_int, [C.c_void_p]),
+    "gbApplyBoundaryConditions": (C.c_int, [MeshP]),
     "gbBatchFree": (None, [C.c_void_p]),
     "gbBatchInitUniform": (C.c_int, [C.c_void_p, C.c_int, gb_vector, C.c_float, C.c_float]),
     "gbBatchSetState": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]),

@@ -89,11 +89,27 @@ struct RunGraphs {
     }
 };
 
+struct FieldImpl;
+
+// Boundary conditions that FvmEulerSlipBc / FvmEulerInletOutletBc have been
+// asked for and that have not been applied yet.  They are applied together,
+// by one k_bc_table launch, before anything reads or writes the fields'
+// device values (the next FvmEulerStepPrepare in the reference's loop); each
+// ghost's state depends only on its interior cell's, so this is bitwise what
+// applying each call at once gives, a later condition on a region replacing
+// an earlier one as it overwrote it.
+struct PendingBcs {
+    FvmField* f[3] = {nullptr, nullptr, nullptr};   // rho, rhou, rhoe
+    GhostBcTable t{};
+    bool any = false;
+};
+
 struct MeshImpl {
     Topology topo;
     Numbering num;
     DevMesh dev;
     uint32_t* d_cell_new = nullptr;   // old -> new, N+G
+    PendingBcs pending;
     RunGraphs euler_run, nsi_run;
     cudaStream_t capture = nullptr;   // stream the loops are captured on
     double* h_result = nullptr;       // pinned: FvmFieldReduceSum's value on the host
@@ -398,6 +414,60 @@ void enqueue_farfield(cuMesh* mesh, FvmField* rho, FvmField* rhou, FvmField* rho
                        make_float3(mach.x, mach.y, mach.z), p, t, s);
 }
 
+// Applies the deferred boundary conditions of the mesh, if any.
+bool flush_bcs(cuMesh* mesh) {
+    MeshImpl* mi = impl(mesh);
+    if (!mi || !mi->pending.any) return true;
+    PendingBcs& pb = mi->pending;
+    for (int k = 0; k < 2; ++k) {
+        pb.t.rho[k] = (float*)impl(pb.f[0])->val[k];
+        pb.t.rhou[k] = (float4*)impl(pb.f[1])->val[k];
+        pb.t.rhoe[k] = (float*)impl(pb.f[2])->val[k];
+    }
+    pb.any = false;
+    launch_bc_table(mi->dev, pb.t, impl(pb.f[0])->cur, t_stream);
+    return launch_ok("boundary conditions");
+}
+
+// Applies them when f is one of the fields they are for.
+bool flush_for(const FvmField* f) {
+    FieldImpl* fi = impl(f);
+    if (!fi || !fi->bound) return true;
+    cuMesh* mesh = const_cast<cuMesh*>(fi->bound);
+    const PendingBcs& pb = impl(mesh)->pending;
+    if (pb.any && (pb.f[0] == f || pb.f[1] == f || pb.f[2] == f)) return flush_bcs(mesh);
+    return true;
+}
+
+// Records a boundary condition of region r (type 0 slip, 1 far field);
+// false when the mesh has more regions than the table holds (the caller
+// then applies it at once).
+bool defer_bc(cuMesh* mesh, FvmField* rho, FvmField* rhou, FvmField* rhoe, int r, int type, gb_vector mach, float p,
+              float temp, bool* ok) {
+    MeshImpl* mi = impl(mesh);
+    const int n_regions = (int)mi->topo.regions.size();
+    *ok = true;
+    if (n_regions > kMaxBcRegions) return false;
+    PendingBcs& pb = mi->pending;
+    if (pb.any && (pb.f[0] != rho || pb.f[1] != rhou || pb.f[2] != rhoe)) *ok = flush_bcs(mesh);
+    if (!pb.any) {
+        pb.f[0] = rho;
+        pb.f[1] = rhou;
+        pb.f[2] = rhoe;
+        pb.t = GhostBcTable{};
+        pb.t.n = n_regions;
+        pb.t.store = 1;
+        for (int k = 0; k <= n_regions; ++k) pb.t.start[k] = mi->num.region_start[k];
+        for (int k = 0; k < n_regions; ++k) pb.t.type[k] = -1;
+        pb.any = true;
+    }
+    pb.t.type[r] = type;
+    pb.t.mach[r] = make_float3(mach.x, mach.y, mach.z);
+    pb.t.p[r] = p;
+    pb.t.temp[r] = temp;
+    return true;
+}
+
 // store_gradients = false: only the face states the flux needs are written
 EulerGrad grad_of(FvmField* rho, FvmField* rhou, FvmField* rhoe, bool store_gradients) {
     return EulerGrad{store_gradients ? impl(rho)->grad : nullptr, store_gradients ? impl(rhou)->grad : nullptr,
@@ -594,6 +664,7 @@ bool mesh_access(cuMesh* mesh, MeshAccess* out) {
 bool field_access(FvmField* f, cuMesh* mesh, int comps, FieldAccess* out) {
     FieldImpl* fi = impl(f);
     if (!fi || !fi->val[0]) { set_error("null or unallocated field"); return false; }
+    if (!flush_for(f)) return false;
     if (mesh ? !bind(mesh, f, comps, "field") : fi->comps != comps) {
         if (!mesh) set_error("field has the wrong number of components");
         return false;
@@ -735,6 +806,7 @@ void FvmFieldFree(FvmField* f) {
     if (!f) return;
     FieldImpl* fi = impl(f);
     if (fi) {
+        flush_for(f);
         dfree(fi->val[0]); dfree(fi->val[1]); dfree(fi->grad); dfree(fi->partials); dfree(fi->staging);
         if (fi->rec) cudaFree(fi->rec);
         delete fi;
@@ -762,19 +834,19 @@ void* FvmFieldValueIndex(FvmField* v, size_t i) {
 
 void VarGpuToCpu(FvmField* var) {
     clear_error();
-    if (var && impl(var)) download_values(var);
+    if (var && impl(var) && flush_for(var)) download_values(var);
 }
 
 void VarAllGpuToCpu(FvmField* var) {
     clear_error();
-    if (var && impl(var) && download_values(var)) download_gradients(var);
+    if (var && impl(var) && flush_for(var) && download_values(var)) download_gradients(var);
 }
 
 int gbVarCpuToGpu(cuMesh* mesh, FvmField* var) {
     clear_error();
     if (!check_mesh(mesh)) return 1;
     FieldImpl* fi = impl(var);
-    if (!fi || !bind(mesh, var, fi->comps, "gbVarCpuToGpu") || !ensure_staging(fi)) return 1;
+    if (!fi || !bind(mesh, var, fi->comps, "gbVarCpuToGpu") || !flush_for(var) || !ensure_staging(fi)) return 1;
     cudaStream_t s = t_stream;
     const uint32_t* idx = impl(mesh)->d_cell_new;
     if (!cuda_ok(cudaMemcpyAsync(fi->staging, var->_cpu->value, fi->size * fi->comps * 4, cudaMemcpyHostToDevice, s),
@@ -792,7 +864,7 @@ int FvmEulerInit(cuMesh* mesh, FvmField* rho, FvmField* rhou, FvmField* rhoe, gb
                  gb_scalar temperature) {
     clear_error();
     if (!check_mesh(mesh) || !bind(mesh, rho, 1, "FvmEulerInit") || !bind(mesh, rhou, 3, "FvmEulerInit") ||
-        !bind(mesh, rhoe, 1, "FvmEulerInit"))
+        !bind(mesh, rhoe, 1, "FvmEulerInit") || !flush_bcs(mesh))
         return 1;
     // euler_init, src/models/euler.cu:401-404
     const float r = pressure / temperature;
@@ -813,6 +885,8 @@ int FvmEulerSlipBc(cuMesh* mesh, FvmField* rho, FvmField* rhou, FvmField* rhoe, 
     if (!euler_fields(mesh, rho, rhou, rhoe, "FvmEulerSlipBc")) return 1;
     const int r = region_lookup(mesh, region);
     if (r < 0) return 1;
+    bool ok = true;
+    if (defer_bc(mesh, rho, rhou, rhoe, r, 0, gb_vector{0.f, 0.f, 0.f}, 0.f, 0.f, &ok)) return ok ? 0 : 1;
     enqueue_slip(mesh, rho, rhou, rhoe, r, impl(rho)->cur, t_stream);
     return launch_ok("FvmEulerSlipBc") ? 0 : 1;
 }
@@ -823,13 +897,21 @@ int FvmEulerInletOutletBc(cuMesh* mesh, FvmField* rho, FvmField* rhou, FvmField*
     if (!euler_fields(mesh, rho, rhou, rhoe, "FvmEulerInletOutletBc")) return 1;
     const int r = region_lookup(mesh, region);
     if (r < 0) return 1;
+    bool ok = true;
+    if (defer_bc(mesh, rho, rhou, rhoe, r, 1, mach, pressure, temperature, &ok)) return ok ? 0 : 1;
     enqueue_farfield(mesh, rho, rhou, rhoe, r, impl(rho)->cur, mach, pressure, temperature, t_stream);
     return launch_ok("FvmEulerInletOutletBc") ? 0 : 1;
 }
 
+int gbApplyBoundaryConditions(cuMesh* mesh) {
+    clear_error();
+    if (!check_mesh(mesh)) return 1;
+    return flush_bcs(mesh) ? 0 : 1;
+}
+
 int FvmEulerStepPrepare(cuMesh* mesh, FvmField* rho, FvmField* rhou, FvmField* rhoe) {
     clear_error();
-    if (!euler_fields(mesh, rho, rhou, rhoe, "FvmEulerStepPrepare")) return 1;
+    if (!euler_fields(mesh, rho, rhou, rhoe, "FvmEulerStepPrepare") || !flush_bcs(mesh)) return 1;
     if (!ensure_grad(mesh, rho) || !ensure_grad(mesh, rhou) || !ensure_grad(mesh, rhoe)) return 1;
     launch_grad_lim(impl(mesh)->dev, state_of(rho, rhou, rhoe, impl(rho)->cur), grad_of(rho, rhou, rhoe, true),
                     g_transposed.load() != 0, t_stream);
@@ -844,7 +926,9 @@ int FvmEulerStep(cuMesh* mesh, FvmField* rho, FvmField* rhou, FvmField* rhoe, gb
         set_error("FvmEulerStep: only the \"steady\" scheme exists");
         return 1;
     }
-    if (!euler_fields(mesh, rho, rhou, rhoe, "FvmEulerStep") || !bind(mesh, error, 1, "FvmEulerStep")) return 1;
+    if (!euler_fields(mesh, rho, rhou, rhoe, "FvmEulerStep") || !bind(mesh, error, 1, "FvmEulerStep") ||
+        !flush_bcs(mesh))
+        return 1;
     if (!impl(rho)->rec || !impl(rhou)->rec) {
         set_error("FvmEulerStep: call FvmEulerStepPrepare first");
         return 1;
@@ -863,7 +947,7 @@ int FvmEulerStep(cuMesh* mesh, FvmField* rho, FvmField* rhou, FvmField* rhoe, gb
 gb_scalar FvmFieldReduceSum(cuMesh* mesh, FvmField* var) {
     clear_error();
     const float nan = std::numeric_limits<float>::quiet_NaN();
-    if (!check_mesh(mesh) || !bind(mesh, var, 1, "FvmFieldReduceSum")) return nan;
+    if (!check_mesh(mesh) || !bind(mesh, var, 1, "FvmFieldReduceSum") || !flush_for(var)) return nan;
     FieldImpl* fi = impl(var);
     MeshImpl* mi = impl(mesh);
     cudaStream_t s = t_stream;
@@ -890,7 +974,9 @@ int64_t gbEulerRun(cuMesh* mesh, FvmField* rho, FvmField* rhou, FvmField* rhoe, 
                    double* residual_history) {
     clear_error();
     if (n_iter < 0 || n_bc < 0 || (n_bc > 0 && !bcs)) { set_error("gbEulerRun: bad arguments"); return -1; }
-    if (!euler_fields(mesh, rho, rhou, rhoe, "gbEulerRun") || !bind(mesh, error, 1, "gbEulerRun")) return -1;
+    if (!euler_fields(mesh, rho, rhou, rhoe, "gbEulerRun") || !bind(mesh, error, 1, "gbEulerRun") ||
+        !flush_bcs(mesh))
+        return -1;
     MeshImpl* mi = impl(mesh);
     for (int b = 0; b < n_bc; ++b) {
         if (bcs[b].region_id >= mi->topo.regions.size() || (bcs[b].type != 0 && bcs[b].type != 1)) {
@@ -1255,7 +1341,7 @@ int gbFvmGradient(cuMesh* mesh, FvmField* u) {
     clear_error();
     if (!check_mesh(mesh)) return 1;
     FieldImpl* fi = impl(u);
-    if (!fi || !bind(mesh, u, fi->comps, "gbFvmGradient") || !nsi_grad(mesh, u)) return 1;
+    if (!fi || !bind(mesh, u, fi->comps, "gbFvmGradient") || !flush_for(u) || !nsi_grad(mesh, u)) return 1;
     launch_fvm_grad(impl(mesh)->dev, fi->comps, fi->comps == 1 ? (const float*)fi->val[fi->cur] : nullptr,
                     fi->comps == 3 ? (const float4*)fi->val[fi->cur] : nullptr, fi->grad, t_stream);
     return launch_ok("gbFvmGradient") ? 0 : 1;
@@ -1270,11 +1356,11 @@ int gbFvmApply(cuMesh* mesh, int op, FvmField* u, FvmField* phi, gb_vector phi_c
     static const int out_comps[11] = {1, 3, 3, 9, 3, 9, 1, 1, 1, 1, 3};
     static const bool needs_grad[11] = {true, false, true, false, false, false, false, false, true, false, false};
     if (op < 0 || op > 10) { set_error("gbFvmApply: unknown operator"); return 1; }
-    if (!bind(mesh, u, in_comps[op], "gbFvmApply")) return 1;
+    if (!bind(mesh, u, in_comps[op], "gbFvmApply") || !flush_for(u)) return 1;
     if (needs_grad[op] && !fi->grad) { set_error("gbFvmApply: the operator needs the field's gradient (gbFvmGradient)"); return 1; }
     const float4* phi_v = nullptr;
     if (op == 9 || op == 10) {
-        if (!phi || !bind(mesh, phi, 3, "gbFvmApply")) { if (!phi) set_error("gbFvmApply: the operator needs a vector field phi"); return 1; }
+        if (!phi || !bind(mesh, phi, 3, "gbFvmApply") || !flush_for(phi)) { if (!phi) set_error("gbFvmApply: the operator needs a vector field phi"); return 1; }
         phi_v = (const float4*)impl(phi)->val[impl(phi)->cur];
     }
     MeshImpl* mi = impl(mesh);

@@ -170,11 +170,14 @@ int FvmEulerInit(cuMesh* mesh, FvmField* rho, FvmField* rhou, FvmField* rhoe, gb
                  gb_scalar pressure, gb_scalar temperature);
 
 /* Slip wall on a region's ghosts: mirrored momentum, copied density and
- * energy.  src/models/euler.cu:412-442, 552-568. */
+ * energy.  src/models/euler.cu:412-442, 552-568.  Recorded and applied with
+ * the other conditions by the next call that uses the fields on the device
+ * (see gbApplyBoundaryConditions); an unknown region is an error at once. */
 int FvmEulerSlipBc(cuMesh* mesh, FvmField* rho, FvmField* rhou, FvmField* rhoe, const char* region);
 
 /* Far-field ghosts (sub/supersonic inflow/outflow from the interior Mach
- * number and the sign of u.n).  src/models/euler.cu:446-520, 571-593. */
+ * number and the sign of u.n).  src/models/euler.cu:446-520, 571-593.
+ * Recorded like FvmEulerSlipBc. */
 int FvmEulerInletOutletBc(cuMesh* mesh, FvmField* rho, FvmField* rhou, FvmField* rhoe, gb_vector mach,
                           gb_scalar pressure, gb_scalar temperature, const char* region);
 
@@ -235,6 +238,15 @@ typedef struct gbBc {
     gb_scalar pressure;
     gb_scalar temperature;
 } gbBc;
+
+/* FvmEulerSlipBc and FvmEulerInletOutletBc record their condition and return;
+ * all recorded conditions are applied together, in one kernel, by the next
+ * call that reads or writes the fields on the device (FvmEulerStepPrepare in
+ * the reference's loop, VarGpuToCpu, gbVarCpuToGpu, ...), with the results
+ * of applying each at once (each ghost's state depends only on its interior
+ * cell's; a later condition on a region replaces an earlier one).  This
+ * applies them now.  Returns 0, or nonzero on error. */
+int gbApplyBoundaryConditions(cuMesh* mesh);
 
 /* Runs n_iter iterations of the PhysicsEuler::step loop (boundary conditions
  * in the given order, prepare, step, residual sum) as a replayed CUDA graph,
