@@ -56,6 +56,11 @@ class FvmField(C.Structure):
                 ("_gpu", C.POINTER(FvmFieldBase)), ("name", C.c_char_p), ("impl", C.c_void_p)]
 
 
+class gbFvmTerm(C.Structure):
+    _fields_ = [("op", C.c_int), ("coef", C.c_float), ("u", C.POINTER(FvmField)), ("phi", C.POINTER(FvmField)),
+                ("phi_const", gb_vector)]
+
+
 class gbBc(C.Structure):
     _fields_ = [("type", C.c_int), ("region_id", C.c_uint), ("mach", gb_vector), ("pressure", C.c_float),
                 ("temperature", C.c_float)]
@@ -106,6 +111,7 @@ _PROTOS = {
     "gbBatchSetResidualScale": (C.c_int, [C.c_void_p, C.c_int, C.c_double]),
     "gbFvmGradient": (C.c_int, [MeshP, FieldP]),
     "gbFvmApply": (C.c_int, [MeshP, C.c_int, FieldP, FieldP, gb_vector, C.c_void_p]),
+    "gbFvmApplyTerms": (C.c_int, [MeshP, C.c_int, C.POINTER(gbFvmTerm), FieldP]),
     "gbRenderRegionScalar": (C.c_int64, [MeshP, C.c_uint, FieldP, C.c_float, C.c_float, C.c_void_p, C.c_int64]),
     "FieldsWriteVtu": (C.c_int, [C.c_char_p, MeshP, C.POINTER(FieldP), C.c_size_t]),
     "gbFieldsWriteVtuBinary": (C.c_int, [C.c_char_p, MeshP, C.POINTER(FieldP), C.c_size_t]),

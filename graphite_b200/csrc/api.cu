@@ -1347,15 +1347,68 @@ int gbFvmGradient(cuMesh* mesh, FvmField* u) {
     return launch_ok("gbFvmGradient") ? 0 : 1;
 }
 
+}  // extern "C"
+
+namespace {
+// by operator id (GB_FVM_*): components of the input field and of the
+// output, whether the operator reads the input's gradient
+constexpr int kFvmOps = 11;
+const int kOpInComps[kFvmOps] = {1, 1, 1, 3, 1, 3, 3, 1, 1, 1, 3};
+const int kOpOutComps[kFvmOps] = {1, 3, 3, 9, 3, 9, 1, 1, 1, 1, 3};
+const bool kOpNeedsGrad[kFvmOps] = {true, false, true, false, false, false, false, false, true, false, false};
+}  // namespace
+
+extern "C" {
+
+int gbFvmApplyTerms(cuMesh* mesh, int n_terms, const gbFvmTerm* terms, FvmField* out) {
+    clear_error();
+    const char* what = "gbFvmApplyTerms";
+    if (!check_mesh(mesh)) return 1;
+    if (!terms || n_terms < 1 || n_terms > kFvmMaxTerms) {
+        set_error("gbFvmApplyTerms: between 1 and " + std::to_string(kFvmMaxTerms) + " terms");
+        return 1;
+    }
+    FvmTermDev dt[kFvmMaxTerms];
+    int oc = 0;
+    for (int q = 0; q < n_terms; ++q) {
+        const gbFvmTerm& t = terms[q];
+        const std::string tq = "gbFvmApplyTerms: term " + std::to_string(q);
+        if (t.op < 0 || t.op >= kFvmOps) { set_error(tq + ": unknown operator"); return 1; }
+        if (kOpOutComps[t.op] == 9) { set_error(tq + ": tensor-valued operators have no field form"); return 1; }
+        if (q > 0 && kOpOutComps[t.op] != oc) { set_error(tq + ": every term must give the same kind of value"); return 1; }
+        oc = kOpOutComps[t.op];
+        FieldImpl* fi = impl(t.u);
+        if (!fi) { set_error(tq + ": null field"); return 1; }
+        if (!bind(mesh, t.u, kOpInComps[t.op], what) || !flush_for(t.u)) return 1;
+        if (kOpNeedsGrad[t.op] && !fi->grad) { set_error(tq + ": the operator needs the field's gradient (gbFvmGradient)"); return 1; }
+        const float4* phi_v = nullptr;
+        if (t.op == 9 || t.op == 10) {
+            if (!t.phi) { set_error(tq + ": the operator needs a vector field phi"); return 1; }
+            if (!bind(mesh, t.phi, 3, what) || !flush_for(t.phi)) return 1;
+            phi_v = (const float4*)impl(t.phi)->val[impl(t.phi)->cur];
+        }
+        if (out == t.u || out == t.phi) { set_error(tq + ": the output field is also an input"); return 1; }
+        dt[q] = FvmTermDev{t.op, t.coef, fi->comps == 1 ? (const float*)fi->val[fi->cur] : nullptr,
+                           fi->comps == 3 ? (const float4*)fi->val[fi->cur] : nullptr, fi->grad, phi_v,
+                           make_float3(t.phi_const.x, t.phi_const.y, t.phi_const.z)};
+    }
+    if (!out) { set_error("gbFvmApplyTerms: null output field"); return 1; }
+    if (!bind(mesh, out, oc, what) || !flush_for(out)) return 1;
+    FieldImpl* fo = impl(out);
+    launch_fvm_terms(impl(mesh)->dev, oc, n_terms, dt, oc == 1 ? (float*)fo->val[fo->cur] : nullptr,
+                     oc == 3 ? (float4*)fo->val[fo->cur] : nullptr, t_stream);
+    return launch_ok(what) ? 0 : 1;
+}
+
 int gbFvmApply(cuMesh* mesh, int op, FvmField* u, FvmField* phi, gb_vector phi_const, float* out) {
     clear_error();
     if (!check_mesh(mesh) || !out) { if (!out) set_error("gbFvmApply: null output"); return 1; }
     FieldImpl* fi = impl(u);
     if (!fi) { set_error("gbFvmApply: null field"); return 1; }
-    static const int in_comps[11] = {1, 1, 1, 3, 1, 3, 3, 1, 1, 1, 3};
-    static const int out_comps[11] = {1, 3, 3, 9, 3, 9, 1, 1, 1, 1, 3};
-    static const bool needs_grad[11] = {true, false, true, false, false, false, false, false, true, false, false};
-    if (op < 0 || op > 10) { set_error("gbFvmApply: unknown operator"); return 1; }
+    const int* in_comps = kOpInComps;
+    const int* out_comps = kOpOutComps;
+    const bool* needs_grad = kOpNeedsGrad;
+    if (op < 0 || op >= kFvmOps) { set_error("gbFvmApply: unknown operator"); return 1; }
     if (!bind(mesh, u, in_comps[op], "gbFvmApply") || !flush_for(u)) return 1;
     if (needs_grad[op] && !fi->grad) { set_error("gbFvmApply: the operator needs the field's gradient (gbFvmGradient)"); return 1; }
     const float4* phi_v = nullptr;

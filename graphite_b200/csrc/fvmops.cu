@@ -1,31 +1,14 @@
-// The reference's generic finite-volume operators (include/fvmops.cuh:96-219)
-// on the renumbered layout, and the least-squares gradient + limiter of any
-// scalar or vector field (ScalarVarComputeGradient / VectorVarComputeGradient
-// and the limiter pass, src/fvmops.cu:51-266).
-//
-// Every operator is a per-cell sum over the cell's faces (fvmOpSetup,
-// include/fvmops.cuh:33-48): with c1 the neighbour across the face,
-// d0 = face centre - c0, d1 = face centre - c1, n the face normal oriented
-// away from c0 and ds = face area / volume of c0.  A ghost neighbour carries
-// its interior cell's gradient and limiter (fvmScalGradLimBc,
-// src/fvmops.cu:272-304).  Tensors are stored as the reference's
-// tensor{u, v, w}: outer(a, b) = (a b.x, a b.y, a b.z).
-#include "euler_ops.cuh"
+// Launches of the reference's generic finite-volume operators
+// (include/fvmops.cuh:96-219; the operators themselves are the device
+// functors of fvm_ops.cuh): one operator over every interior cell, or a
+// linear combination of operators in one pass over each cell's faces; and the
+// least-squares gradient + limiter of any scalar or vector field
+// (ScalarVarComputeGradient / VectorVarComputeGradient and the limiter pass,
+// src/fvmops.cu:51-266).
+#include "fvm_ops.cuh"
 
 namespace gb {
 namespace {
-
-struct OpIn {
-    const float* s;        // scalar values (N+G) or null
-    const float4* v;       // vector values (N+G) or null
-    const float4* g;       // gradients + limiters: N (scalar) or 3N (vector)
-    const float4* phi;     // per-cell vector field (convection ops) or null
-    float3 phi_c;          // constant vector (convection ops)
-};
-
-__device__ __forceinline__ float3 gvec(const float4* g, uint32_t c, int a, int comps) {
-    return f3(__ldg(&g[comps * c + a]));
-}
 
 template <int COMPS>
 __global__ void k_fvm_grad(MeshDev m, const float* __restrict__ s, const float4* __restrict__ v, float4* grad) {
@@ -66,103 +49,73 @@ __global__ void k_fvm_grad(MeshDev m, const float* __restrict__ s, const float4*
 }
 
 // out: planar, out[q * N + i] for component q of cell i
-__global__ void k_fvm_apply(MeshDev m, int op, OpIn in, float* __restrict__ out) {
+__device__ __forceinline__ void store_planar(float* out, uint32_t N, uint32_t i, float x) { out[i] = x; }
+__device__ __forceinline__ void store_planar(float* out, uint32_t N, uint32_t i, float3 x) {
+    out[i] = x.x; out[N + i] = x.y; out[2 * N + i] = x.z;
+}
+__device__ __forceinline__ void store_planar(float* out, uint32_t N, uint32_t i, const fvm::Tens3& x) {
+#pragma unroll
+    for (int b = 0; b < 3; ++b) store_planar(out + 3 * b * (size_t)N, N, i, x.r[b]);
+}
+
+template <class Op>
+__global__ void k_fvm_op(MeshDev m, Op op, float* __restrict__ out) {
     const uint32_t c0 = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c0 >= m.N) return;
-    float x[9];
-#pragma unroll
-    for (int q = 0; q < 9; ++q) x[q] = 0.f;
-    const int comps = in.v ? 3 : 1;
-    const uint32_t nf = __ldg(&m.nfc[c0]);
-    for (uint32_t k = c0; k < c0 + nf * m.N; k += m.N) {
-        const uint32_t c1 = __ldg(&m.nbc[k]);
-        const uint32_t t = __ldg(&m.twin[k]);
-        const bool ghost = t >= m.S;
-        const uint32_t g1 = ghost ? c0 : c1;            // gradient owner of the neighbour
-        const float4 gk = __ldg(&m.cf_geo[k]);
-        const float3 n = f3(gk);
-        const float ds = gk.w;
-        const float3 d0 = f3(__ldg(&m.df[k]));
-        const float3 fc = f3(__ldg(&m.face_geo[2 * __ldg(&m.nb[k]).x + 1]));
-        const float3 d1 = ghost ? fc - f3(__ldg(&m.cell_geo[c1])) : f3(__ldg(&m.df[t]));
-        if (comps == 1) {
-            const float u0 = __ldg(&in.s[c0]), u1 = __ldg(&in.s[c1]);
-            switch (op) {
-                case 0: {   // fvmLaplacianC: dot(grad c1 + grad c0, n) / 2 ds
-                    x[0] += dot(gvec(in.g, g1, 0, 1) + gvec(in.g, c0, 0, 1), n) * 0.5f * ds;
-                    break;
-                }
-                case 1: {   // fvmScalGradC
-                    const float phi = norm(d0) / norm(d0 - d1);
-                    const float3 r = n * ((u1 * phi + u0 * (1.f - phi)) * ds);
-                    x[0] += r.x; x[1] += r.y; x[2] += r.z;
-                    break;
-                }
-                case 2: {   // fvmScalGradCCorrect (face centre taken as is, as the reference does)
-                    const float phi = norm(d0) / norm(d0 - d1);
-                    const float3 d_err = fc - (d0 - d1) * phi;
-                    const float3 r = n * (dot(gvec(in.g, c0, 0, 1), d_err) * ds);
-                    x[0] += r.x; x[1] += r.y; x[2] += r.z;
-                    break;
-                }
-                case 4: {   // fvmBoundScalGradC
-                    const float3 r = n * ((u1 - u0) * ds);
-                    x[0] += r.x; x[1] += r.y; x[2] += r.z;
-                    break;
-                }
-                case 7: case 8: {   // fvmConvConstScalU / fvmConvConstScalU2
-                    float a = u0, b = u1;
-                    if (op == 8) {
-                        const float4 ga = __ldg(&in.g[c0]), gb = __ldg(&in.g[g1]);
-                        a = u0 + dot(f3(ga), d0) * ga.w;
-                        b = u1 + dot(f3(gb), d1) * gb.w;
-                    }
-                    const float an = dot(n, in.phi_c);
-                    x[0] += ((an * a + an * b) - fmaxf(fabsf(an), fabsf(an)) * (b - a)) * 0.5f * ds;
-                    break;
-                }
-                case 9: {   // fvmConvScalU
-                    const float a0 = dot(n, f3(__ldg(&in.phi[c0]))), a1 = dot(n, f3(__ldg(&in.phi[c1])));
-                    x[0] += ((a0 * u0 + a1 * u1) - fmaxf(fabsf(a0), fabsf(a1)) * (u1 - u0)) * 0.5f * ds;
-                    break;
-                }
-                default: break;
-            }
-        } else {
-            const float3 u0 = f3(__ldg(&in.v[c0])), u1 = f3(__ldg(&in.v[c1]));
-            switch (op) {
-                case 3: {   // fvmVecGradC: outer(n, u1 phi + u0 (1 - phi)) ds
-                    const float l0 = norm(d0), l1 = norm(d1);
-                    const float phi = l0 / (l0 + l1);
-                    const float3 w = (u1 * phi + u0 * (1.f - phi)) * ds;
-                    const float wc[3] = {w.x, w.y, w.z};
-#pragma unroll
-                    for (int b = 0; b < 3; ++b) { x[3 * b] += n.x * wc[b]; x[3 * b + 1] += n.y * wc[b]; x[3 * b + 2] += n.z * wc[b]; }
-                    break;
-                }
-                case 5: {   // fvmBoundVecGradC: outer(u1 - u0, n) ds
-                    const float3 du = (u1 - u0) * ds;
-                    const float nc[3] = {n.x, n.y, n.z};
-#pragma unroll
-                    for (int b = 0; b < 3; ++b) { x[3 * b] += du.x * nc[b]; x[3 * b + 1] += du.y * nc[b]; x[3 * b + 2] += du.z * nc[b]; }
-                    break;
-                }
-                case 6: {   // fvmDivC
-                    x[0] += dot(u0 + u1, n) * 0.5f * ds;
-                    break;
-                }
-                case 10: {  // fvmConvVecU (the dissipation takes max(a0, a1), not of |a|, as the reference does)
-                    const float a0 = dot(n, f3(__ldg(&in.phi[c0]))), a1 = dot(n, f3(__ldg(&in.phi[c1])));
-                    const float3 r = ((u0 * a0 + u1 * a1) - (u1 - u0) * fmaxf(a0, a1)) * (0.5f * ds);
-                    x[0] += r.x; x[1] += r.y; x[2] += r.z;
-                    break;
-                }
-                default: break;
-            }
+    if (c0 < m.N) store_planar(out, m.N, c0, fvm::cell_sum(m, c0, op));
+}
+
+// One term of a linear combination of operators (gbFvmApplyTerms).
+struct TermDev {
+    int op;
+    float coef;
+    const float* s;
+    const float4* v;
+    const float4* g;
+    const float4* phi;
+    float3 phi_c;
+};
+struct TermList {
+    int n;
+    TermDev t[kFvmMaxTerms];
+};
+
+// the face contribution of term t (operators of the output type of OUT)
+template <int OUT>
+__device__ __forceinline__ void term_contrib(const TermDev& t, const fvm::OpFace& f, float& x1, float3& x3) {
+    using namespace fvm;
+    if (OUT == 1) {
+        switch (t.op) {
+            case 0: x1 = x1 + LaplacianC{t.g}.contrib(f) * t.coef; break;
+            case 6: x1 = x1 + DivC{t.v}.contrib(f) * t.coef; break;
+            case 7: x1 = x1 + ConvConstScal<false>{t.s, t.g, t.phi_c}.contrib(f) * t.coef; break;
+            case 8: x1 = x1 + ConvConstScal<true>{t.s, t.g, t.phi_c}.contrib(f) * t.coef; break;
+            case 9: x1 = x1 + ConvScalU{t.s, t.phi}.contrib(f) * t.coef; break;
+            default: break;
+        }
+    } else {
+        switch (t.op) {
+            case 1: x3 = x3 + ScalGradC{t.s}.contrib(f) * t.coef; break;
+            case 2: x3 = x3 + ScalGradCCorrect{t.g}.contrib(f) * t.coef; break;
+            case 4: x3 = x3 + BoundScalGradC{t.s}.contrib(f) * t.coef; break;
+            case 10: x3 = x3 + ConvVecU{t.v, t.phi}.contrib(f) * t.coef; break;
+            default: break;
         }
     }
-    const int oc = (op == 3 || op == 5) ? 9 : ((op == 1 || op == 2 || op == 4 || op == 10) ? 3 : 1);
-    for (int q = 0; q < oc; ++q) out[(size_t)q * m.N + c0] = x[q];
+}
+
+// sum of coef x operator over the terms, one pass over each cell's faces,
+// into the interior cells of a scalar (OUT = 1) or vector (OUT = 3) field
+template <int OUT>
+__global__ void k_fvm_terms(MeshDev m, TermList terms, float* __restrict__ out_s, float4* __restrict__ out_v) {
+    const uint32_t c0 = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c0 >= m.N) return;
+    float x1 = 0.f;
+    float3 x3 = make_float3(0.f, 0.f, 0.f);
+    fvm::for_each_face(m, c0, [&](const fvm::OpFace& f) {
+        for (int q = 0; q < terms.n; ++q) term_contrib<OUT>(terms.t[q], f, x1, x3);
+    });
+    if (OUT == 1) out_s[c0] = x1;
+    else out_v[c0] = make_float4(x3.x, x3.y, x3.z, 0.f);
 }
 
 inline unsigned grid_n(int64_t n) { return (unsigned)((n + kBlock - 1) / kBlock); }
@@ -181,7 +134,35 @@ void launch_fvm_grad(const DevMesh& m, int comps, const float* s, const float4* 
 void launch_fvm_apply(const DevMesh& m, int op, const float* s, const float4* v, const float4* g, const float4* phi,
                       float3 phi_c, float* out, cudaStream_t st) {
     if (m.N == 0) return;
-    k_fvm_apply<<<grid_n(m.N), kBlock, 0, st>>>(mesh_dev(m), op, OpIn{s, v, g, phi, phi_c}, out);
+    using namespace fvm;
+    const MeshDev md = mesh_dev(m);
+    const unsigned gn = grid_n(m.N);
+    switch (op) {
+        case 0: k_fvm_op<<<gn, kBlock, 0, st>>>(md, LaplacianC{g}, out); break;
+        case 1: k_fvm_op<<<gn, kBlock, 0, st>>>(md, ScalGradC{s}, out); break;
+        case 2: k_fvm_op<<<gn, kBlock, 0, st>>>(md, ScalGradCCorrect{g}, out); break;
+        case 3: k_fvm_op<<<gn, kBlock, 0, st>>>(md, VecGradC{v}, out); break;
+        case 4: k_fvm_op<<<gn, kBlock, 0, st>>>(md, BoundScalGradC{s}, out); break;
+        case 5: k_fvm_op<<<gn, kBlock, 0, st>>>(md, BoundVecGradC{v}, out); break;
+        case 6: k_fvm_op<<<gn, kBlock, 0, st>>>(md, DivC{v}, out); break;
+        case 7: k_fvm_op<<<gn, kBlock, 0, st>>>(md, ConvConstScal<false>{s, g, phi_c}, out); break;
+        case 8: k_fvm_op<<<gn, kBlock, 0, st>>>(md, ConvConstScal<true>{s, g, phi_c}, out); break;
+        case 9: k_fvm_op<<<gn, kBlock, 0, st>>>(md, ConvScalU{s, phi}, out); break;
+        case 10: k_fvm_op<<<gn, kBlock, 0, st>>>(md, ConvVecU{v, phi}, out); break;
+        default: return;
+    }
+    count_launch();
+}
+
+void launch_fvm_terms(const DevMesh& m, int out_comps, int n_terms, const FvmTermDev* terms, float* out_s,
+                      float4* out_v, cudaStream_t st) {
+    if (m.N == 0) return;
+    TermList tl{};
+    tl.n = n_terms;
+    for (int q = 0; q < n_terms; ++q)
+        tl.t[q] = TermDev{terms[q].op, terms[q].coef, terms[q].s, terms[q].v, terms[q].g, terms[q].phi, terms[q].phi_c};
+    if (out_comps == 1) k_fvm_terms<1><<<grid_n(m.N), kBlock, 0, st>>>(mesh_dev(m), tl, out_s, nullptr);
+    else k_fvm_terms<3><<<grid_n(m.N), kBlock, 0, st>>>(mesh_dev(m), tl, nullptr, out_v);
     count_launch();
 }
 

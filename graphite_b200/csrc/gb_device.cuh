@@ -173,6 +173,21 @@ void launch_reduce_final(int n_partials, const double* partials, double* out, cu
                          RunCtl* ctl = nullptr, double* history = nullptr, unsigned long long history_cap = 0,
                          double tolerance = 0.0);
 
+// One term coef x operator of gbFvmApplyTerms, on device arrays (fvmops.cu).
+constexpr int kFvmMaxTerms = 8;
+struct FvmTermDev {
+    int op;
+    float coef;
+    const float* s;       // scalar input values (N + G) or null
+    const float4* v;      // vector input values (N + G) or null
+    const float4* g;      // the scalar input's gradients + limiters (N) or null
+    const float4* phi;    // velocity field (N + G) or null
+    float3 phi_c;         // constant velocity
+};
+// out_comps 1: out_s[i] = the sum at interior cell i; 3: out_v[i]
+void launch_fvm_terms(const DevMesh& m, int out_comps, int n_terms, const FvmTermDev* terms, float* out_s,
+                      float4* out_v, cudaStream_t st);
+
 // permute helpers for host transfers (new <-> reference order)
 void launch_gather_scalar(int64_t n, const float* src, const uint32_t* idx, float* dst, cudaStream_t s);
 void launch_gather_vector(int64_t n, const float4* src, const uint32_t* idx, float* dst3, cudaStream_t s);

@@ -153,7 +153,7 @@ def solve_warm(batch, ws_per_instance: Sequence[Optional[WarmStart]], cases: Seq
         batch.set_residual_scale(i, 0.0)
     _, _, _, _, hist = batch.run(cfl, 1, history=True)
     res0 = hist[:, 0].copy()
-    # 2. predicted states, judged by their residual
+    # 2. predicted states, measured against the cold first residual
     for i, (m, p, t) in enumerate(cases):
         batch.set_residual_scale(i, float(res0[i]))
         if ws_per_instance[i] is not None:

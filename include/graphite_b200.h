@@ -451,6 +451,24 @@ enum {
 int gbFvmGradient(cuMesh* mesh, FvmField* u);
 int gbFvmApply(cuMesh* mesh, int op, FvmField* u, FvmField* phi, gb_vector phi_const, float* out);
 
+/* gbFvmApplyTerms: sum over terms of coef x operator at every interior cell,
+ * the operators composed in one pass over each cell's faces (as a model
+ * kernel composes the reference's inline operators), into the interior
+ * values of `out` on the device: a scalar field when the operators give
+ * scalars, a vector field when they give vectors (tensor-valued operators
+ * have no field form).  Ghost values of `out` are left as they are; `out`
+ * must not be an input of any term.  1 to 8 terms, all of one output kind;
+ * an operator that needs a gradient reads its input's (gbFvmGradient).
+ * Returns 0, or 1 with gbGetLastError() set. */
+typedef struct gbFvmTerm {
+    int op;                /* GB_FVM_* */
+    gb_scalar coef;        /* multiplies the operator */
+    FvmField* u;           /* input field */
+    FvmField* phi;         /* velocity field of GB_FVM_CONV_SCAL / GB_FVM_CONV_VEC, else NULL */
+    gb_vector phi_const;   /* constant velocity of GB_FVM_CONV_CONST_SCAL / _SCAL2 */
+} gbFvmTerm;
+int gbFvmApplyTerms(cuMesh* mesh, int n_terms, const gbFvmTerm* terms, FvmField* out);
+
 /* ---- Incompressible Navier-Stokes (artificial compressibility) ----
  * The reference's NSI model (src/models/nsi.cu:71,114,137,144) calls
  * FvmNSIInit, FvmNSISlipBc, FvmNSIInletOutletBc, FvmNSIStepPrepare and

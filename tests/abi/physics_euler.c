@@ -43,6 +43,8 @@ static int layout(void) {
     FIELD(gbBc, type); FIELD(gbBc, region_id); FIELD(gbBc, mach); FIELD(gbBc, pressure);
     FIELD(gbBc, temperature);
     FIELD(gbBatchInstance, mesh); FIELD(gbBatchInstance, n_bc); FIELD(gbBatchInstance, bcs);
+    FIELD(gbFvmTerm, op); FIELD(gbFvmTerm, coef); FIELD(gbFvmTerm, u); FIELD(gbFvmTerm, phi);
+    FIELD(gbFvmTerm, phi_const);
     printf("gb_vector sizeof %zu\n", sizeof(gb_vector));
     printf("gb_tensor sizeof %zu\n", sizeof(gb_tensor));
     printf("cuMeshBase sizeof %zu\n", sizeof(cuMeshBase));
@@ -51,6 +53,7 @@ static int layout(void) {
     printf("FvmField sizeof %zu\n", sizeof(FvmField));
     printf("gbBc sizeof %zu\n", sizeof(gbBc));
     printf("gbBatchInstance sizeof %zu\n", sizeof(gbBatchInstance));
+    printf("gbFvmTerm sizeof %zu\n", sizeof(gbFvmTerm));
     return 0;
 }
 

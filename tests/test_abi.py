@@ -23,7 +23,7 @@ LIBDIR = os.path.join(ROOT, "graphite_b200")
 
 # Field order of the reference's structs (include/mesh.cuh:18-63,
 # include/fvmfields.cuh:16-30, include/datatypes.cuh:36-54); the gb structs
-# are this library's own (gbBc, gbBatchInstance).
+# are this library's own (gbBc, gbBatchInstance, gbFvmTerm).
 ORDER = {
     "gb_vector": ["x", "y", "z"],
     "gb_tensor": ["u", "v", "w"],
@@ -36,10 +36,11 @@ ORDER = {
     "FvmField": ["_cpu", "_hgpu", "_gpu", "name", "impl"],
     "gbBc": ["type", "region_id", "mach", "pressure", "temperature"],
     "gbBatchInstance": ["mesh", "n_bc", "bcs"],
+    "gbFvmTerm": ["op", "coef", "u", "phi", "phi_const"],
 }
 CTYPES = {"gb_vector": capi.gb_vector, "gb_tensor": capi.gb_tensor, "cuMeshBase": capi.cuMeshBase,
           "cuMesh": capi.cuMesh, "FvmFieldBase": capi.FvmFieldBase, "FvmField": capi.FvmField, "gbBc": capi.gbBc,
-          "gbBatchInstance": capi.gbBatchInstance}
+          "gbBatchInstance": capi.gbBatchInstance, "gbFvmTerm": capi.gbFvmTerm}
 
 
 @pytest.fixture(scope="module")

@@ -102,3 +102,76 @@ def test_operators_match_reference_operators(su2_paths, workdir, name):
     for f in (fs, fv, fp):
         lib.FvmFieldFree(f)
     lib.cuMeshFree(mesh)
+
+
+SCALAR_TERMS = [(9, -1.0), (0, 0.3), (6, 0.5), (8, 2.0), (7, -0.25)]
+VECTOR_TERMS = [(1, 1.0), (4, -1.0), (10, 0.7), (2, 0.2)]
+
+
+@pytest.mark.parametrize("name", ["tet_6x3x2", "prism_6x3x2", "hex_6x3x2", "pyramid_6x3x2"])
+def test_operator_terms_compose_in_one_pass(su2_paths, workdir, name):
+    """gbFvmApplyTerms (several operators summed in one pass over the faces,
+    into a field on the device) against the same linear combination of the
+    reference's own operators (tests/golden/<mesh>_fvmops.npz) and of
+    gbFvmApply's single-operator results; and its argument checks."""
+    from test_oracle_golden import FVMOP_SLOTS, VECTOR_OPS
+
+    lib = capi.load()
+    z = np.load(f"{cases.__file__.rsplit('/', 1)[0]}/{name}_fvmops.npz")
+    fvm = str(workdir / f"{name}_terms.fvm")
+    capi.check(lib.cuMeshFromSu2(su2_paths(name).encode(), fvm.encode()), "cuMeshFromSu2")
+    mesh = lib.cuMeshFromFile(fvm.encode())
+    n = int(lib.cuMeshGetVarSize(mesh))
+    N = int(lib.cuMeshGetnCells(mesh))
+    fs, fv, fp = _field(lib, mesh, n, 1, b"s", z["s"]), _field(lib, mesh, n, 3, b"v", z["v"]), \
+        _field(lib, mesh, n, 3, b"phi", z["phi"])
+    capi.check(lib.gbFvmGradient(mesh, fs), "gbFvmGradient")
+    ops = z["ops"].reshape(N, 35).astype(np.float64)
+    pc = capi.vec(tuple(float(c) for c in z["phi_const"]))
+    out_s = lib.FvmFieldNew(4, n, b"r", 0)
+    out_v = lib.FvmFieldNew(12, n, b"rv", 0)
+
+    def terms(spec):
+        arr = (capi.gbFvmTerm * len(spec))()
+        for q, (op, coef) in enumerate(spec):
+            arr[q] = capi.gbFvmTerm(op, coef, fv if op in VECTOR_OPS else fs, fp if op in (9, 10) else None, pc)
+        return arr
+
+    for spec, out, k in ((SCALAR_TERMS, out_s, 1), (VECTOR_TERMS, out_v, 3)):
+        capi.check(lib.gbFvmApplyTerms(mesh, len(spec), terms(spec), out), "gbFvmApplyTerms")
+        lib.VarGpuToCpu(out)
+        got = capi.field_values(out)[:N].reshape(N, k)
+        ref = np.zeros((N, k))
+        single = np.zeros((N, k))
+        scale = 0.0
+        for op, coef in spec:
+            o, w = FVMOP_SLOTS[op]
+            assert w == k
+            ref += coef * ops[:, o:o + k]
+            scale += abs(coef) * np.max(np.abs(ops[:, o:o + k]))
+            one = np.zeros((N, k), np.float32)
+            u = fv if op in VECTOR_OPS else fs
+            capi.check(lib.gbFvmApply(mesh, op, u, fp, pc, one.ctypes.data), f"gbFvmApply {op}")
+            single += coef * one
+        assert np.max(np.abs(got - ref)) <= 1e-4 * scale, np.max(np.abs(got - ref)) / scale
+        assert np.max(np.abs(got - single)) <= 2e-6 * scale, np.max(np.abs(got - single)) / scale
+
+    # argument checks: every one returns 1 with an error and launches nothing
+    bad = [
+        (terms([(0, 1.0), (1, 1.0)]), 2, out_s),        # a scalar and a vector operator
+        (terms([(3, 1.0)]), 1, out_v),                   # tensor-valued
+        (terms([(0, 1.0)]), 1, out_v),                   # scalar terms into a vector field
+        (terms([(0, 1.0)]), 1, fs),                      # the output is an input
+        (terms([(0, 1.0)]), 0, out_s),                   # no terms
+        (terms([(0, 1.0)] * 9), 9, out_s),               # more than 8
+        (terms([(11, 1.0)]), 1, out_s),                  # unknown operator
+    ]
+    no_phi = (capi.gbFvmTerm * 1)()
+    no_phi[0] = capi.gbFvmTerm(9, 1.0, fs, None, pc)
+    bad.append((no_phi, 1, out_s))                       # convection by a missing velocity field
+    for arr, cnt, out in bad:
+        assert lib.gbFvmApplyTerms(mesh, cnt, arr, out) == 1
+        assert capi.last_error()
+    for f in (fs, fv, fp, out_s, out_v):
+        lib.FvmFieldFree(f)
+    lib.cuMeshFree(mesh)
