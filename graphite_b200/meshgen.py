@@ -226,9 +226,12 @@ def channel_bump(nx: int = 60, ny: int = 20, nz: int = 4, length: float = 3.0, h
                  width: float = 0.2, bump_height: float = 0.1, cells: str = "tet") -> ElementMesh:
     """Channel [0,L]x[0,H]x[0,W] with a circular-arc bump of chord 1 on x in [1,2].
 
-    ``cells`` = "tet" (6 tets per hex), "hex", "prism" (2 per hex) or
-    "pyramid" (6 pyramids per hex around a centre node).  Regions: inlet,
-    outlet, lower (bump wall), upper, sides.
+    ``cells`` = "tet" (6 tets per hex), "hex", "prism" (2 per hex),
+    "pyramid" (6 pyramids per hex around a centre node), "mixed" (hexes,
+    prisms and pyramids in thirds of the columns along x: every face between
+    them is a whole quad on both sides) or "layered" (prisms in the lower
+    half of the z layers, tets above: the prisms' triangles are cut along the
+    tets' diagonal).  Regions: inlet, outlet, lower (bump wall), upper, sides.
     """
     xs = np.linspace(0.0, length, nx + 1)
     r = (0.25 + bump_height ** 2) / (2 * bump_height) if bump_height > 0 else 0.0
@@ -249,26 +252,40 @@ def channel_bump(nx: int = 60, ny: int = 20, nz: int = 4, length: float = 3.0, h
     # node_index's first axis must not wrap: pad so (i + 1) % n0 is i + 1.
     pad = np.concatenate([node_index, node_index[:1]], axis=0)
     corners = _hex_corner_ids(pad, cells_ijk)
-    if cells == "tet":
-        blocks = [(TET, _kuhn_tets(corners))]
-    elif cells == "hex":
+    def hexes(cs):
         order = [(0, 0, 0), (1, 0, 0), (1, 1, 0), (0, 1, 0), (0, 0, 1), (1, 0, 1), (1, 1, 1), (0, 1, 1)]
-        blocks = [(HEX, np.stack([corners[:, a, b, c] for a, b, c in order], axis=1))]
-    elif cells == "prism":
-        blocks = [(PRISM, _prisms(corners))]
-    elif cells == "pyramid":
-        centres = nodes[corners.reshape(-1, 8)].mean(axis=1)
-        cid = nodes.shape[0] + np.arange(corners.shape[0])
-        nodes = np.concatenate([nodes, _f32(centres)])
+        return np.stack([cs[:, a, b, c] for a, b, c in order], axis=1)
+
+    def pyramids(nodes, cs):
+        centres = nodes[cs.reshape(-1, 8)].mean(axis=1)
+        cid = nodes.shape[0] + np.arange(cs.shape[0])
         quads = [[(0, 0, 0), (1, 0, 0), (1, 1, 0), (0, 1, 0)], [(0, 0, 1), (0, 1, 1), (1, 1, 1), (1, 0, 1)],
                  [(0, 0, 0), (0, 0, 1), (1, 0, 1), (1, 0, 0)], [(0, 1, 0), (1, 1, 0), (1, 1, 1), (0, 1, 1)],
                  [(0, 0, 0), (0, 1, 0), (0, 1, 1), (0, 0, 1)], [(1, 0, 0), (1, 0, 1), (1, 1, 1), (1, 1, 0)]]
-        pyr = np.empty((corners.shape[0], 6, 5), dtype=np.int64)
+        pyr = np.empty((cs.shape[0], 6, 5), dtype=np.int64)
         for q, quad in enumerate(quads):
             for v, (a, b, c) in enumerate(quad):
-                pyr[:, q, v] = corners[:, a, b, c]
+                pyr[:, q, v] = cs[:, a, b, c]
             pyr[:, q, 4] = cid
-        blocks = [(PYRAMID, pyr.reshape(-1, 5))]
+        return np.concatenate([nodes, _f32(centres)]), pyr.reshape(-1, 5)
+
+    if cells == "tet":
+        blocks = [(TET, _kuhn_tets(corners))]
+    elif cells == "hex":
+        blocks = [(HEX, hexes(corners))]
+    elif cells == "prism":
+        blocks = [(PRISM, _prisms(corners))]
+    elif cells == "pyramid":
+        nodes, pyr = pyramids(nodes, corners)
+        blocks = [(PYRAMID, pyr)]
+    elif cells == "mixed":
+        col = cells_ijk[:, 0]
+        zone = np.where(col < nx // 3, 0, np.where(col < 2 * nx // 3, 1, 2))
+        nodes, pyr = pyramids(nodes, corners[zone == 2])
+        blocks = [(HEX, hexes(corners[zone == 0])), (PRISM, _prisms(corners[zone == 1])), (PYRAMID, pyr)]
+    elif cells == "layered":
+        low = cells_ijk[:, 2] < max(nz // 2, 1)
+        blocks = [(PRISM, _prisms(corners[low])), (TET, _kuhn_tets(corners[~low]))]
     else:
         raise ValueError(cells)
     ii, jj, kk = np.meshgrid(np.arange(nx + 1), np.arange(ny + 1), np.arange(nz + 1), indexing="ij")

@@ -35,6 +35,8 @@ MESHES = {
     "hex_6x3x2": lambda: meshgen.channel_bump(6, 3, 2, cells="hex"),
     "prism_6x3x2": lambda: meshgen.channel_bump(6, 3, 2, cells="prism"),
     "pyramid_6x3x2": lambda: meshgen.channel_bump(6, 3, 2, cells="pyramid"),
+    "mixed_6x3x2": lambda: meshgen.channel_bump(6, 3, 2, cells="mixed"),
+    "layered_6x3x2": lambda: meshgen.channel_bump(6, 3, 2, cells="layered"),
     "tet_12x6x2": lambda: meshgen.channel_bump(12, 6, 2, cells="tet"),
     "channel": lambda: meshgen.channel_bump(60, 20, 4, cells="tet"),
 }

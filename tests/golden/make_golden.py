@@ -45,10 +45,11 @@ import refio  # noqa: E402
 DRIVER = os.path.join(ROOT, "oracle", "_ref", "ref_driver")
 FVMOPS = os.path.join(ROOT, "oracle", "_ref", "ref_fvmops")
 
-METRICS = ["tet_6x3x2", "hex_6x3x2", "prism_6x3x2", "pyramid_6x3x2", "tet_12x6x2"]
-PREPARE = ["tet_6x3x2", "hex_6x3x2", "prism_6x3x2", "pyramid_6x3x2", "tet_12x6x2"]
+MIXED = ["mixed_6x3x2", "layered_6x3x2"]     # several element kinds in one mesh
+METRICS = ["tet_6x3x2", "hex_6x3x2", "prism_6x3x2", "pyramid_6x3x2", "tet_12x6x2"] + MIXED
+PREPARE = ["tet_6x3x2", "hex_6x3x2", "prism_6x3x2", "pyramid_6x3x2", "tet_12x6x2"] + MIXED
 SOLVES = [("tet_12x6x2", 20000), ("channel", 2000), ("channel", 40000)]
-FVMOPS_MESHES = ["tet_6x3x2", "prism_6x3x2", "hex_6x3x2", "pyramid_6x3x2"]
+FVMOPS_MESHES = ["tet_6x3x2", "prism_6x3x2", "hex_6x3x2", "pyramid_6x3x2"] + MIXED
 PHI_CONST = (0.7, -0.2, 0.4)
 
 
@@ -86,8 +87,10 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--out", default=HERE)
     ap.add_argument("--work", default=os.path.join(tempfile.gettempdir(), "graphite_b200_golden_work"))
-    ap.add_argument("--only", default="", help="comma list of metrics,prepare,solve")
+    ap.add_argument("--only", default="", help="comma list of metrics,prepare,solve,fvmops")
+    ap.add_argument("--cases", default="", help="comma list of mesh names (default: all of each kind)")
     a = ap.parse_args()
+    pick = set(a.cases.split(",")) if a.cases else None
     os.makedirs(a.out, exist_ok=True)
     os.makedirs(a.work, exist_ok=True)
     only = set(a.only.split(",")) if a.only else {"metrics", "prepare", "solve", "fvmops"}
@@ -106,6 +109,8 @@ def main():
     bcs = cases.channel_bcs()
     if "metrics" in only:
         for name in METRICS:
+            if pick is not None and name not in pick:
+                continue
             m, path = su2(name)
             case = os.path.join(a.work, f"{name}_metrics.txt")
             refio.write_case(case, init, bcs)
@@ -118,6 +123,8 @@ def main():
                                 **{k: rec[k] for k in FLOAT_KEYS_METRICS + INT_KEYS_METRICS})
     if "prepare" in only:
         for name in PREPARE:
+            if pick is not None and name not in pick:
+                continue
             m, path = su2(name)
             rho, rhou, rhoe = cases.synthetic_state(m)
             state = os.path.join(a.work, f"{name}_state.bin")
@@ -132,6 +139,8 @@ def main():
                                 state_rho=rho, state_rhou=rhou, state_rhoe=rhoe, **keep)
     if "solve" in only:
         for name, iters in SOLVES:
+            if pick is not None and name not in pick:
+                continue
             m, path = su2(name)
             case = os.path.join(a.work, f"{name}_solve{iters}.txt")
             refio.write_case(case, init, bcs, cfl=0.8, iters=iters)
@@ -144,6 +153,8 @@ def main():
             print(name, iters, txt.strip().splitlines()[-1])
     if "fvmops" in only:
         for name in FVMOPS_MESHES:
+            if pick is not None and name not in pick:
+                continue
             m, path = su2(name)
             sf, vf, pf = operator_fields(m)
             fields = os.path.join(a.work, f"{name}_fvmops_fields.bin")

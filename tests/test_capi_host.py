@@ -30,7 +30,7 @@ def test_struct_layout_matches_header():
     assert C.sizeof(capi.gbBc) == 4 + 4 + 12 + 4 + 4
 
 
-@pytest.mark.parametrize("name", ["tet_6x3x2", "hex_6x3x2", "prism_6x3x2", "pyramid_6x3x2", "tet_12x6x2"])
+@pytest.mark.parametrize("name", ["tet_6x3x2", "hex_6x3x2", "prism_6x3x2", "pyramid_6x3x2", "mixed_6x3x2", "layered_6x3x2", "tet_12x6x2"])
 def test_converter_matches_reference_converter(name, su2_paths, workdir):
     """cuMeshFromSu2 writes the file the reference's converter writes: same
     float32 nodes, same faces with the same node order, same cells (face
@@ -54,7 +54,8 @@ def test_converter_matches_reference_converter(name, su2_paths, workdir):
 
 
 @pytest.mark.parametrize("cells,shape", [("tet", (60, 30, 20)), ("hex", (60, 40, 60)), ("prism", (60, 30, 40)),
-                                         ("pyramid", (60, 30, 13))])
+                                         ("pyramid", (60, 30, 13)), ("mixed", (60, 30, 30)),
+                                         ("layered", (60, 30, 20))])
 def test_parallel_converter_matches_oracle_topology(workdir, cells, shape):
     """With 130k-216k elements the converter builds the face records, sorts
     them and numbers the faces on several host threads; its file equals the

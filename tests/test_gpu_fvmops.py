@@ -65,7 +65,7 @@ def test_operators_match_restatement(su2_paths, workdir, name):
     lib.cuMeshFree(mesh)
 
 
-@pytest.mark.parametrize("name", ["tet_6x3x2", "prism_6x3x2", "hex_6x3x2", "pyramid_6x3x2"])
+@pytest.mark.parametrize("name", ["tet_6x3x2", "prism_6x3x2", "hex_6x3x2", "pyramid_6x3x2", "mixed_6x3x2", "layered_6x3x2"])
 def test_operators_match_reference_operators(su2_paths, workdir, name):
     """gbFvmGradient and gbFvmApply against the reference's own operators and
     gradients (tests/golden/<mesh>_fvmops.npz, made by oracle/ref_fvmops.cu on
@@ -108,7 +108,7 @@ SCALAR_TERMS = [(9, -1.0), (0, 0.3), (6, 0.5), (8, 2.0), (7, -0.25)]
 VECTOR_TERMS = [(1, 1.0), (4, -1.0), (10, 0.7), (2, 0.2)]
 
 
-@pytest.mark.parametrize("name", ["tet_6x3x2", "prism_6x3x2", "hex_6x3x2", "pyramid_6x3x2"])
+@pytest.mark.parametrize("name", ["tet_6x3x2", "prism_6x3x2", "hex_6x3x2", "pyramid_6x3x2", "mixed_6x3x2", "layered_6x3x2"])
 def test_operator_terms_compose_in_one_pass(su2_paths, workdir, name):
     """gbFvmApplyTerms (several operators summed in one pass over the faces,
     into a field on the device) against the same linear combination of the

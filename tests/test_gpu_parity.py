@@ -19,7 +19,7 @@ from oracle import OracleMesh, OracleSolver
 
 pytestmark = pytest.mark.gpu
 
-SMALL = ["tet_6x3x2", "hex_6x3x2", "prism_6x3x2", "pyramid_6x3x2", "tet_12x6x2"]
+SMALL = ["tet_6x3x2", "hex_6x3x2", "prism_6x3x2", "pyramid_6x3x2", "mixed_6x3x2", "layered_6x3x2", "tet_12x6x2"]
 BCS = cases.channel_bcs()
 INIT = (cases.CHANNEL_MACH, cases.P_INF, cases.T_INF)
 

@@ -12,7 +12,7 @@ import cases
 from helpers import face_map, rel_max
 from oracle import OracleMesh, OracleSolver
 
-METRIC_MESHES = ["tet_6x3x2", "hex_6x3x2", "prism_6x3x2", "pyramid_6x3x2", "tet_12x6x2"]
+METRIC_MESHES = ["tet_6x3x2", "hex_6x3x2", "prism_6x3x2", "pyramid_6x3x2", "mixed_6x3x2", "layered_6x3x2", "tet_12x6x2"]
 
 # float32 fast-math reference vs float64 restatement: relative to the
 # array's max magnitude.  Volumes and LSQ inverses lose a few more bits to
@@ -109,7 +109,7 @@ FVMOP_SLOTS = {0: (0, 1), 1: (1, 3), 2: (4, 3), 3: (7, 9), 4: (16, 3), 5: (19, 9
 VECTOR_OPS = (3, 5, 6, 10)
 
 
-@pytest.mark.parametrize("name", ["tet_6x3x2", "prism_6x3x2", "hex_6x3x2", "pyramid_6x3x2"])
+@pytest.mark.parametrize("name", ["tet_6x3x2", "prism_6x3x2", "hex_6x3x2", "pyramid_6x3x2", "mixed_6x3x2", "layered_6x3x2"])
 def test_operator_restatement_matches_reference_operators(name):
     """oracle/fvmops_oracle.py against the reference's own inline fvmOp
     functions (include/fvmops.cuh:96-219) evaluated by oracle/ref_fvmops.cu
