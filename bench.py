@@ -362,6 +362,9 @@ def run_ours(args, rank, world, local_rank):
     cyl = None
     if rank == 0 and world == 1 and not args.skip_cylinder:
         cyl = run_cylinder(args, dev_stream)
+    lift = None
+    if rank == 0 and world == 1 and args.lift_history:
+        lift = run_lift_history(args, dev_stream)
 
     # ---- CPU baseline (rank 0, N = 1) ----
     cpu = None
@@ -392,8 +395,74 @@ def run_ours(args, rank, world, local_rank):
         "incompressible_cylinder_re40": cyl,
         "cpu_baseline": cpu,
     }
+    if lift is not None:
+        out["lift_history"] = lift
     case.close()
     return out
+
+
+def run_lift_history(args, dev_stream, n_cases=4, every=10):
+    """Whether any stopping rule can hold lift to 1e-4 on the warm-start
+    airfoil: the first n_cases held-out draws of the warm-start experiment
+    (120k airfoil, CFL 0.5) run for args.lift_history iterations from the
+    uniform start, and again from a start one ulp higher in every interior
+    density; lift every `every` iterations.  Reports per case the residual
+    ratio to the first iteration's (lowest and last), the lift's spread over the last 5,000
+    iterations, its means over consecutive 10,000-iteration windows and the
+    change between the last two, and the two runs' lift difference at a few
+    iterations -- all relative to |lift| of the last window's mean."""
+    import torch
+    from graphite_b200 import meshgen
+    from graphite_b200.euler import EulerCase, lift_drag
+
+    cache = os.path.join(tempfile.gettempdir(), "graphite_b200_bench")
+    os.makedirs(cache, exist_ok=True)
+    path = os.path.join(cache, "airfoil_120000.su2")
+    if not os.path.exists(path):
+        tmp = path + f".tmp{os.getpid()}"
+        meshgen.airfoil_extruded(120_000).write_su2(tmp)
+        os.replace(tmp, path)
+    rng = np.random.default_rng(WARM_SEED)
+    draws = [(float(rng.uniform(0.3, 0.8)), float(rng.uniform(-4.0, 8.0))) for _ in range(WARM_TRAIN + WARM_HELD)]
+    iters = (args.lift_history // every) * every
+    window = 10_000 // every
+    out = []
+    with EulerCase(path) as c:
+        for m, a in draws[WARM_TRAIN:WARM_TRAIN + n_cases]:
+            mv, bcs = airfoil_case(m, a)
+            runs = []
+            for perturb in (False, True):
+                c.init(mv, P_INF, T_INF)
+                if perturb:
+                    r, u, e = c.fields()
+                    r = r.copy()
+                    r[: c.n_cells] = np.nextafter(r[: c.n_cells], np.float32(np.inf))
+                    c.set_state(r, u, e)
+                lift, res = [], []
+                for _ in range(iters // every):
+                    h = c.run(bcs, SWEEP_CFL, every, check_every=every)
+                    if not res:
+                        res.append(float(h[0]))      # the first iteration's residual
+                    res.append(float(h[-1]))
+                    lift.append(lift_drag(c.wall_force("wing"), mv)[0])
+                runs.append((np.array(lift), np.array(res)))
+            (l0, r0), (l1, _) = runs
+            means = [float(np.mean(l0[j:j + window])) for j in range(0, len(l0) - window + 1, window)]
+            scale = abs(means[-1]) if means else float(np.max(np.abs(l0)))
+            tail = l0[-min(len(l0), 5000 // every):]
+            at = [k for k in (2000, 5000, 10000, 20000, 40000) if k <= iters]
+            out.append({
+                "mach": m, "aoa_deg": a,
+                "residual_ratio_min": float(np.min(r0) / r0[0]), "residual_ratio_last": float(r0[-1] / r0[0]),
+                "lift_last": float(l0[-1]),
+                "lift_spread_last_5000": float((tail.max() - tail.min()) / scale),
+                "lift_window_means": [x / scale for x in means],
+                "last_window_change": abs(means[-1] - means[-2]) / scale if len(means) > 1 else None,
+                "ulp_start_lift_difference": {str(k): float(abs(l0[k // every - 1] - l1[k // every - 1]) / scale)
+                                              for k in at}})
+    return {"mesh": "airfoil 120k prisms", "cfl": SWEEP_CFL, "iterations": iters, "every": every,
+            "cases": out,
+            "normalisation": "relative to |mean lift| over the last 10,000-iteration window"}
 
 
 CPU_BLOCK = 65536   # cells per oracle call in the CPU legs
@@ -891,6 +960,9 @@ def main():
     ap.add_argument("--skip-batch", action="store_true", help="skip the batched 64-instance airfoil sweep")
     ap.add_argument("--skip-warm", action="store_true", help="skip the learned warm start (train + evaluate)")
     ap.add_argument("--skip-cylinder", action="store_true", help="skip the incompressible cylinder (Re 40)")
+    ap.add_argument("--lift-history", type=int, default=0, metavar="ITERS",
+                    help="also run the lift-history study of the first held-out warm-start cases for ITERS "
+                         "iterations (off by default)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
