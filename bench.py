@@ -383,6 +383,8 @@ def run_ours(args, rank, world, local_rank):
         "gpu_launches": int(launches),
         "roofline": {"bound": "hbm", "kernel": dominant, "achieved": achieved, "peak": peak,
                      "peak_source": peak_kind, "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
+                     "traffic_source": "dram__bytes_read.sum + dram__bytes_write.sum of one ncu capture of this "
+                                       "per-call launch on this workload, recorded in profiles/ncu_traffic.txt",
                      "algorithmic_bytes_per_launch": bm[dominant], "ms_per_launch": t_dom,
                      "other_kernel": {"name": GRAD_KERNEL if dominant == "k_flux" else "k_flux",
                                       "ms_per_launch": t_prep if dominant == "k_flux" else t_flux,
