@@ -140,3 +140,35 @@ def test_batch_warm_start_state_round_trip(meshes):
         r, u, e = b.get_state(1)
         assert np.array_equal(r, rho) and np.array_equal(u, rhou) and np.array_equal(e, rhoe)
     cs[0].close()
+
+
+@pytest.mark.parametrize("tuning", [(256, 1), (256, 5), (1024, 9)])
+def test_batch_on_3d_mixed_meshes_equals_plain_solves(su2_paths, tuning):
+    """A batch over three 3-D channels -- tets, the hex / prism / pyramid mix
+    and prism layers under tets (cells of 4, 5 and 6 faces in one launch; not
+    ghost-heavy, so the plain solves apply the conditions with the ghost
+    kernel while the batch applies them inside its gradient pass) -- follows
+    the plain solves bit for bit."""
+    lib = capi.load()
+    lib.gbSetReferenceMomentumReconstruction(1)
+    names = ["tet_12x6x2", "mixed_6x3x2", "layered_6x3x2"]
+    cs = [EulerCase(su2_paths(n)) for n in names]
+    inst = [(k, mach) for k in range(3) for mach in (0.4, 0.6)]
+    spec = [(k, cases.channel_bcs((m, 0.0, 0.0))) for k, m in inst]
+    with EulerBatch(cs, spec) as b:
+        b.set_tuning(*tuning)
+        for i, (k, m) in enumerate(inst):
+            b.init_uniform(i, (m, 0.0, 0.0), cases.P_INF, cases.T_INF)
+        done, its, rat, st = b.run(0.8, 120)
+        assert done == 120 and np.all(its == 120)
+        got = [b.get_state(i) for i in range(len(inst))]
+    for i, (k, m) in enumerate(inst):
+        c = cs[k]
+        c.init((m, 0.0, 0.0), cases.P_INF, cases.T_INF)
+        h = c.run(cases.channel_bcs((m, 0.0, 0.0)), 0.8, 120)
+        ref = c.fields()
+        for q in range(3):
+            assert np.array_equal(got[i][q], ref[q]), (names[k], m, q)
+        np.testing.assert_allclose(rat[i], h[-1] / h[0], rtol=1e-12)
+    for c in cs:
+        c.close()
