@@ -179,10 +179,11 @@ def load():
 
 
 def header_functions() -> List[str]:
-    """Names of the functions include/graphite_b200.h declares."""
+    """Names of the functions include/graphite_b200.h declares for the library
+    to export (its static inline helpers are defined in the header itself)."""
     text = open(HEADER).read()
     text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
-    names = re.findall(r"^[A-Za-z_][\w\s\*]*?\b([A-Za-z_]\w*)\s*\(", text, flags=re.M)
+    names = re.findall(r"^(?!static\b)[A-Za-z_][\w\s\*]*?\b([A-Za-z_]\w*)\s*\(", text, flags=re.M)
     return sorted(set(n for n in names if n not in ("defined",)))
 
 

@@ -138,6 +138,28 @@ unsigned int cuMeshGetRegionId(cuMesh* mesh, const char* name);
 /* Prints the mesh sizes, src/meshio.cu:8-21. */
 void cuMeshPrintInfo(cuMesh* mesh);
 
+/* CSR views of a host mirror (mesh->_cpu, reference order), the reference's
+ * inline helpers include/mesh.cuh:83-141: the nodes of face i; the faces of
+ * cell i and, in the same pattern, the cells across them (a ghost cell has
+ * one face, its boundary face); the ghost count of region r. */
+static inline unsigned int* cuMeshGetFaceStart(cuMeshBase* m, int i) { return m->face_nodes + m->face_nodes_starts[i]; }
+static inline unsigned int* cuMeshGetFaceEnd(cuMeshBase* m, int i) { return m->face_nodes + m->face_nodes_starts[i + 1]; }
+static inline unsigned int cuMeshGetFaceSize(cuMeshBase* m, int i) {
+    return m->face_nodes_starts[i + 1] - m->face_nodes_starts[i];
+}
+static inline unsigned int* cuMeshGetCellStart(cuMeshBase* m, int i) { return m->cell_faces + m->cell_faces_starts[i]; }
+static inline unsigned int* cuMeshGetCellEnd(cuMeshBase* m, int i) { return m->cell_faces + m->cell_faces_starts[i + 1]; }
+static inline unsigned int cuMeshGetCellSize(cuMeshBase* m, int i) {
+    return m->cell_faces_starts[i + 1] - m->cell_faces_starts[i];
+}
+static inline unsigned int* cuMeshGetCellConnect(cuMeshBase* m, int i) {
+    return m->cell_connects + m->cell_faces_starts[i];
+}
+static inline unsigned int cuMeshGetGhostCellFace(cuMeshBase* m, int i) { return m->cell_faces[m->cell_faces_starts[i]]; }
+static inline unsigned int cuMeshGetRegionSize(cuMeshBase* m, unsigned int r) {
+    return m->ghost_cell_starts[r + 1] - m->ghost_cell_starts[r];
+}
+
 /* -------------------------------------------------------------- fields --- */
 
 /* A field of `size` elements of `elem_size` bytes (sizeof(gb_scalar) or

@@ -13,7 +13,9 @@
  *       boundary conditions in PhysicsEuler's sorted-key order,
  *       FvmEulerStepPrepare, FvmEulerStep and FvmFieldReduceSum; prints
  *       "residual <i> <value>" per iteration and, after VarGpuToCpu, the
- *       interior density as "rho <i> <value>" lines.
+ *       interior density as "rho <i> <value>" lines; before the loop, the
+ *       host mirror's faces, cells (faces:neighbours) and region ghost counts
+ *       through the header's CSR helpers ("face", "cell", "region" lines).
  */
 #include <stddef.h>
 #include <stdio.h>
@@ -72,6 +74,22 @@ static int run(const char* su2, const char* fvm, int iterations) {
     cuMesh* mesh = cuMeshFromFile(fvm);
     if (!mesh) { fprintf(stderr, "cuMeshFromFile: %s\n", gbGetLastError()); return 1; }
     const size_t n = cuMeshGetVarSize(mesh);
+    /* the host mirror through the header's CSR helpers */
+    cuMeshBase* hb = mesh->_cpu;
+    for (int i = 0; i < (int)hb->n_faces; ++i) {
+        printf("face %d %u", i, cuMeshGetFaceSize(hb, i));
+        for (const unsigned int* q = cuMeshGetFaceStart(hb, i); q != cuMeshGetFaceEnd(hb, i); ++q) printf(" %u", *q);
+        printf("\n");
+    }
+    for (int i = 0; i < (int)n; ++i) {
+        printf("cell %d %u", i, cuMeshGetCellSize(hb, i));
+        const unsigned int* c = cuMeshGetCellConnect(hb, i);
+        for (const unsigned int* q = cuMeshGetCellStart(hb, i); q != cuMeshGetCellEnd(hb, i); ++q, ++c)
+            printf(" %u:%u", *q, *c);
+        if (i >= (int)hb->n_cells) printf(" ghostface %u", cuMeshGetGhostCellFace(hb, i));
+        printf("\n");
+    }
+    for (unsigned int r = 0; r < (unsigned int)hb->n_regions; ++r) printf("region %u %u\n", r, cuMeshGetRegionSize(hb, r));
     FvmField* rho = FvmFieldNew(sizeof(gb_scalar), n, "rho", 1);
     FvmField* rhou = FvmFieldNew(sizeof(gb_vector), n, "rhou", 1);
     FvmField* rhoe = FvmFieldNew(sizeof(gb_scalar), n, "rhoe", 1);

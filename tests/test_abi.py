@@ -87,11 +87,30 @@ def test_c_caller_runs_the_physics_euler_loop(exe, su2_paths, tmp_path):
     r = subprocess.run([exe, "run", path, str(tmp_path / "m.fvm"), str(iters)], capture_output=True, text=True,
                        timeout=300)
     assert r.returncode == 0, r.stderr
-    res = np.array([float(l.split()[2]) for l in r.stdout.splitlines() if l.startswith("residual")], np.float32)
+    lines = r.stdout.splitlines()
+    res = np.array([float(l.split()[2]) for l in lines if l.startswith("residual")], np.float32)
     rho = np.array([float(l.split()[2]) for l in r.stdout.splitlines() if l.startswith("rho")], np.float32)
     assert len(res) == iters
     bcs = cases.channel_bcs()
     with EulerCase(path) as c:
+        # the header's inline CSR helpers read the host mirror as the arrays say
+        fs, fn = capi.mesh_array(c.mesh, "face_nodes_starts"), capi.mesh_array(c.mesh, "face_nodes")
+        faces = [l.split()[2:] for l in lines if l.startswith("face ")]
+        assert len(faces) == len(fs) - 1
+        for i, f in enumerate(faces):
+            assert int(f[0]) == fs[i + 1] - fs[i] and [int(x) for x in f[1:]] == list(fn[fs[i]:fs[i + 1]])
+        cs, cf = capi.mesh_array(c.mesh, "cell_faces_starts"), capi.mesh_array(c.mesh, "cell_faces")
+        cc = capi.mesh_array(c.mesh, "cell_connects")
+        cells = [l.split()[2:] for l in lines if l.startswith("cell ")]
+        assert len(cells) == len(cs) - 1
+        for i, x in enumerate(cells):
+            pairs = [tuple(int(y) for y in p.split(":")) for p in x[1:1 + int(x[0])]]
+            assert pairs == list(zip(cf[cs[i]:cs[i + 1]], cc[cs[i]:cs[i + 1]]))
+            if "ghostface" in x:
+                assert int(x[-1]) == cf[cs[i]]
+        gs = capi.mesh_array(c.mesh, "ghost_cell_starts")
+        regions = [int(l.split()[2]) for l in lines if l.startswith("region ")]
+        assert regions == list(np.diff(gs))
         c.init(cases.CHANNEL_MACH, cases.P_INF, cases.T_INF)
         py = np.array([c.iterate(bcs, 0.8) for _ in range(iters)], np.float32)
         py_rho = c.fields()[0][: c.n_cells]
