@@ -112,6 +112,9 @@ _PROTOS = {
     "gbFvmGradient": (C.c_int, [MeshP, FieldP]),
     "gbFvmApply": (C.c_int, [MeshP, C.c_int, FieldP, FieldP, gb_vector, C.c_void_p]),
     "gbFvmApplyTerms": (C.c_int, [MeshP, C.c_int, C.POINTER(gbFvmTerm), FieldP]),
+    "gbFieldInit": (C.c_int, [MeshP, FieldP, gb_vector]),
+    "gbFieldBcFixed": (C.c_int, [MeshP, FieldP, gb_vector, C.c_uint]),
+    "gbFieldBcZeroGrad": (C.c_int, [MeshP, FieldP, C.c_uint]),
     "gbRenderRegionScalar": (C.c_int64, [MeshP, C.c_uint, FieldP, C.c_float, C.c_float, C.c_void_p, C.c_int64]),
     "FieldsWriteVtu": (C.c_int, [C.c_char_p, MeshP, C.POINTER(FieldP), C.c_size_t]),
     "gbFieldsWriteVtuBinary": (C.c_int, [C.c_char_p, MeshP, C.POINTER(FieldP), C.c_size_t]),

@@ -1331,11 +1331,50 @@ int gbNSIWallForce(cuMesh* mesh, FvmField* velocity, FvmField* pressure, unsigne
 // Generic finite-volume operators (fvmops.cu).
 namespace gb {
 void launch_fvm_grad(const DevMesh& m, int comps, const float* s, const float4* v, float4* grad, cudaStream_t st);
+void launch_field_init(int64_t n, int comps, void* val0, void* val1, float4 value, int64_t n_grad, float4* grad,
+                       cudaStream_t st);
+void launch_field_bc(const DevMesh& m, uint32_t g0, uint32_t g1, int comps, int zero_grad, int cur, void* val0,
+                     void* val1, float4 value, cudaStream_t st);
 void launch_fvm_apply(const DevMesh& m, int op, const float* s, const float4* v, const float4* g, const float4* phi,
                       float3 phi_c, float* out, cudaStream_t st);
 }  // namespace gb
 
 extern "C" {
+
+int gbFieldInit(cuMesh* mesh, FvmField* u, gb_vector value) {
+    clear_error();
+    if (!check_mesh(mesh)) return 1;
+    FieldImpl* fi = impl(u);
+    if (!fi || !bind(mesh, u, fi->comps, "gbFieldInit") || !flush_for(u)) return 1;
+    const int64_t n_grad = fi->grad ? impl(mesh)->dev.N * fi->comps : 0;
+    launch_field_init((int64_t)fi->size, fi->comps, fi->val[0], fi->val[1], make_float4(value.x, value.y, value.z, 0.f),
+                      n_grad, fi->grad, t_stream);
+    return launch_ok("gbFieldInit") ? 0 : 1;
+}
+
+static int field_bc(cuMesh* mesh, FvmField* u, unsigned int region_id, int zero_grad, gb_vector value,
+                    const char* what) {
+    clear_error();
+    if (!check_mesh(mesh)) return 1;
+    FieldImpl* fi = impl(u);
+    if (!fi || !bind(mesh, u, fi->comps, what) || !flush_for(u)) return 1;
+    MeshImpl* mi = impl(mesh);
+    if (region_id >= mi->topo.regions.size()) {
+        set_error(std::string(what) + ": no region " + std::to_string(region_id));
+        return 1;
+    }
+    launch_field_bc(mi->dev, mi->num.region_start[region_id], mi->num.region_start[region_id + 1], fi->comps, zero_grad,
+                    fi->cur, fi->val[0], fi->val[1], make_float4(value.x, value.y, value.z, 0.f), t_stream);
+    return launch_ok(what) ? 0 : 1;
+}
+
+int gbFieldBcFixed(cuMesh* mesh, FvmField* u, gb_vector value, unsigned int region_id) {
+    return field_bc(mesh, u, region_id, 0, value, "gbFieldBcFixed");
+}
+
+int gbFieldBcZeroGrad(cuMesh* mesh, FvmField* u, unsigned int region_id) {
+    return field_bc(mesh, u, region_id, 1, gb_vector{0.f, 0.f, 0.f}, "gbFieldBcZeroGrad");
+}
 
 int gbFvmGradient(cuMesh* mesh, FvmField* u) {
     clear_error();

@@ -5,6 +5,8 @@
 // least-squares gradient + limiter of any scalar or vector field
 // (ScalarVarComputeGradient / VectorVarComputeGradient and the limiter pass,
 // src/fvmops.cu:51-266).
+#include <algorithm>
+
 #include "fvm_ops.cuh"
 
 namespace gb {
@@ -118,6 +120,38 @@ __global__ void k_fvm_terms(MeshDev m, TermList terms, float* __restrict__ out_s
     else out_v[c0] = make_float4(x3.x, x3.y, x3.z, 0.f);
 }
 
+// ScalarVarInit / VectorVarInit (src/fvmops.cu:8-44): every value, cells and
+// ghosts, in both buffers; gradients zero with limiter 1 where the field has
+// them.
+__global__ void k_field_init(int64_t n, float* s0, float* s1, float4* v0, float4* v1, float4 value, int64_t n_grad,
+                             float4* grad) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) {
+        if (s0) { s0[i] = value.x; s1[i] = value.x; }
+        else { v0[i] = value; v1[i] = value; }
+    }
+    if (i < n_grad) grad[i] = make_float4(0.f, 0.f, 0.f, 1.f);
+}
+
+// fvmScalarBcFixed (src/fvmops.cu:308-323) and fvmScalarBcZeroGrad /
+// fvmVectorBcZeroGrad (src/fvmops.cu:326-366) on the ghosts [g0, g1) of one
+// region: the given value, or the interior cell's current value, into both
+// buffers.
+__global__ void k_field_bc(uint32_t g0, uint32_t g1, uint32_t N, const uint2* __restrict__ ghost, int zero_grad,
+                           int cur, float* s0, float* s1, float4* v0, float4* v1, float4 value) {
+    const uint32_t t = g0 + blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= g1) return;
+    if (s0) {
+        const float x = zero_grad ? (cur ? s1 : s0)[ghost[t - N].x] : value.x;
+        s0[t] = x;
+        s1[t] = x;
+    } else {
+        const float4 x = zero_grad ? (cur ? v1 : v0)[ghost[t - N].x] : value;
+        v0[t] = x;
+        v1[t] = x;
+    }
+}
+
 inline unsigned grid_n(int64_t n) { return (unsigned)((n + kBlock - 1) / kBlock); }
 
 }  // namespace
@@ -151,6 +185,29 @@ void launch_fvm_apply(const DevMesh& m, int op, const float* s, const float4* v,
         case 10: k_fvm_op<<<gn, kBlock, 0, st>>>(md, ConvVecU{v, phi}, out); break;
         default: return;
     }
+    count_launch();
+}
+
+void launch_field_init(int64_t n, int comps, void* val0, void* val1, float4 value, int64_t n_grad, float4* grad,
+                       cudaStream_t st) {
+    const int64_t m = std::max(n, n_grad);
+    if (m == 0) return;
+    if (comps == 1)
+        k_field_init<<<grid_n(m), kBlock, 0, st>>>(n, (float*)val0, (float*)val1, nullptr, nullptr, value, n_grad, grad);
+    else
+        k_field_init<<<grid_n(m), kBlock, 0, st>>>(n, nullptr, nullptr, (float4*)val0, (float4*)val1, value, n_grad, grad);
+    count_launch();
+}
+
+void launch_field_bc(const DevMesh& m, uint32_t g0, uint32_t g1, int comps, int zero_grad, int cur, void* val0,
+                     void* val1, float4 value, cudaStream_t st) {
+    if (g1 <= g0) return;
+    if (comps == 1)
+        k_field_bc<<<grid_n(g1 - g0), kBlock, 0, st>>>(g0, g1, (uint32_t)m.N, m.ghost, zero_grad, cur, (float*)val0,
+                                                       (float*)val1, nullptr, nullptr, value);
+    else
+        k_field_bc<<<grid_n(g1 - g0), kBlock, 0, st>>>(g0, g1, (uint32_t)m.N, m.ghost, zero_grad, cur, nullptr, nullptr,
+                                                       (float4*)val0, (float4*)val1, value);
     count_launch();
 }
 

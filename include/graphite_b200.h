@@ -473,6 +473,20 @@ enum {
 int gbFvmGradient(cuMesh* mesh, FvmField* u);
 int gbFvmApply(cuMesh* mesh, int op, FvmField* u, FvmField* phi, gb_vector phi_const, float* out);
 
+/* Generic field setup and boundary conditions on the device, for models
+ * built from the operators (a scalar field takes value.x):
+ * gbFieldInit: every value, cells and ghosts, = value; gradients 0 and
+ *   limiters 1 where the field has them (ScalarVarInit / VectorVarInit,
+ *   src/fvmops.cu:8-44);
+ * gbFieldBcFixed: the ghosts of region_id = value (fvmScalarBcFixed,
+ *   src/fvmops.cu:308-323, for vector fields too);
+ * gbFieldBcZeroGrad: each ghost of region_id = its interior cell's value
+ *   (fvmScalarBcZeroGrad / fvmVectorBcZeroGrad, src/fvmops.cu:326-366).
+ * Returns 0, or 1 with gbGetLastError() set (unknown region included). */
+int gbFieldInit(cuMesh* mesh, FvmField* u, gb_vector value);
+int gbFieldBcFixed(cuMesh* mesh, FvmField* u, gb_vector value, unsigned int region_id);
+int gbFieldBcZeroGrad(cuMesh* mesh, FvmField* u, unsigned int region_id);
+
 /* gbFvmApplyTerms: sum over terms of coef x operator at every interior cell,
  * the operators composed in one pass over each cell's faces (as a model
  * kernel composes the reference's inline operators), into the interior

@@ -175,3 +175,53 @@ def test_operator_terms_compose_in_one_pass(su2_paths, workdir, name):
     for f in (fs, fv, fp, out_s, out_v):
         lib.FvmFieldFree(f)
     lib.cuMeshFree(mesh)
+
+
+def test_field_init_and_boundary_conditions(su2_paths, workdir):
+    """gbFieldInit, gbFieldBcFixed and gbFieldBcZeroGrad on a mesh of mixed
+    elements, in the reference's cell order: every value set (gradients
+    zeroed, limiters 1); a region's ghosts set to a value or to their
+    interior cells' values, nothing else touched."""
+    lib = capi.load()
+    fvm = str(workdir / "mixed_fieldbc.fvm")
+    capi.check(lib.cuMeshFromSu2(su2_paths("mixed_6x3x2").encode(), fvm.encode()), "cuMeshFromSu2")
+    mesh = lib.cuMeshFromFile(fvm.encode())
+    n = int(lib.cuMeshGetVarSize(mesh))
+    N = int(lib.cuMeshGetnCells(mesh))
+    rng = np.random.default_rng(7)
+    s = rng.standard_normal(n).astype(np.float32)
+    v = rng.standard_normal((n, 3)).astype(np.float32)
+    fs, fv = _field(lib, mesh, n, 1, b"s", s), _field(lib, mesh, n, 3, b"v", v)
+    capi.check(lib.gbFvmGradient(mesh, fs), "gbFvmGradient")          # the field now has gradients
+    capi.check(lib.gbFieldInit(mesh, fs, capi.vec((2.5, 0.0, 0.0))), "gbFieldInit")
+    lib.VarAllGpuToCpu(fs)
+    assert np.all(capi.field_values(fs) == np.float32(2.5))
+    g, l = capi.field_gradients(fs)
+    assert np.all(g == 0.0) and np.all(np.asarray(l) == 1.0)
+    capi.check(lib.gbFieldInit(mesh, fv, capi.vec((1.0, -2.0, 0.5))), "gbFieldInit")
+    lib.VarGpuToCpu(fv)
+    assert np.array_equal(capi.field_values(fv), np.tile(np.float32([1.0, -2.0, 0.5]), (n, 1)))
+
+    gid, starts = capi.mesh_array(mesh, "ghost_cell_ids"), capi.mesh_array(mesh, "ghost_cell_starts")
+    cfs, cc = capi.mesh_array(mesh, "cell_faces_starts"), capi.mesh_array(mesh, "cell_connects")
+    for f, vals in ((fs, s), (fv, v)):
+        capi.set_field_values(f, vals)
+        capi.check(lib.gbVarCpuToGpu(mesh, f), "gbVarCpuToGpu")
+    r_in, r_low = lib.cuMeshGetRegionId(mesh, b"inlet"), lib.cuMeshGetRegionId(mesh, b"lower")
+    capi.check(lib.gbFieldBcFixed(mesh, fs, capi.vec((7.0, 0.0, 0.0)), r_in), "gbFieldBcFixed")
+    capi.check(lib.gbFieldBcZeroGrad(mesh, fv, r_low), "gbFieldBcZeroGrad")
+    capi.check(lib.gbFieldBcZeroGrad(mesh, fs, r_low), "gbFieldBcZeroGrad")
+    lib.VarGpuToCpu(fs)
+    lib.VarGpuToCpu(fv)
+    want_s, want_v = s.copy(), v.copy()
+    want_s[gid[starts[r_in]:starts[r_in + 1]]] = 7.0
+    low = gid[starts[r_low]:starts[r_low + 1]]
+    inner = cc[cfs[low]]
+    want_s[low] = s[inner]
+    want_v[low] = v[inner]
+    assert np.array_equal(capi.field_values(fs), want_s)
+    assert np.array_equal(capi.field_values(fv), want_v)
+    assert lib.gbFieldBcFixed(mesh, fs, capi.vec((1.0, 0.0, 0.0)), 99) == 1 and capi.last_error()
+    for f in (fs, fv):
+        lib.FvmFieldFree(f)
+    lib.cuMeshFree(mesh)
