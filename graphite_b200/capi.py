@@ -115,6 +115,7 @@ _PROTOS = {
     "gbFieldInit": (C.c_int, [MeshP, FieldP, gb_vector]),
     "gbFieldBcFixed": (C.c_int, [MeshP, FieldP, gb_vector, C.c_uint]),
     "gbFieldBcZeroGrad": (C.c_int, [MeshP, FieldP, C.c_uint]),
+    "gbFieldAxpy": (C.c_int, [MeshP, FieldP, C.c_float, FieldP]),
     "gbRenderRegionScalar": (C.c_int64, [MeshP, C.c_uint, FieldP, C.c_float, C.c_float, C.c_void_p, C.c_int64]),
     "FieldsWriteVtu": (C.c_int, [C.c_char_p, MeshP, C.POINTER(FieldP), C.c_size_t]),
     "gbFieldsWriteVtuBinary": (C.c_int, [C.c_char_p, MeshP, C.POINTER(FieldP), C.c_size_t]),

@@ -1335,6 +1335,7 @@ void launch_field_init(int64_t n, int comps, void* val0, void* val1, float4 valu
                        cudaStream_t st);
 void launch_field_bc(const DevMesh& m, uint32_t g0, uint32_t g1, int comps, int zero_grad, int cur, void* val0,
                      void* val1, float4 value, cudaStream_t st);
+void launch_field_axpy(const DevMesh& m, int comps, float a, const void* x, void* y, cudaStream_t st);
 void launch_fvm_apply(const DevMesh& m, int op, const float* s, const float4* v, const float4* g, const float4* phi,
                       float3 phi_c, float* out, cudaStream_t st);
 }  // namespace gb
@@ -1374,6 +1375,20 @@ int gbFieldBcFixed(cuMesh* mesh, FvmField* u, gb_vector value, unsigned int regi
 
 int gbFieldBcZeroGrad(cuMesh* mesh, FvmField* u, unsigned int region_id) {
     return field_bc(mesh, u, region_id, 1, gb_vector{0.f, 0.f, 0.f}, "gbFieldBcZeroGrad");
+}
+
+int gbFieldAxpy(cuMesh* mesh, FvmField* y, gb_scalar a, FvmField* x) {
+    clear_error();
+    if (!check_mesh(mesh)) return 1;
+    FieldImpl* fy = impl(y);
+    FieldImpl* fx = impl(x);
+    if (!fy || !fx) { set_error("gbFieldAxpy: null field"); return 1; }
+    if (x == y) { set_error("gbFieldAxpy: x and y are the same field"); return 1; }
+    if (!bind(mesh, y, fy->comps, "gbFieldAxpy") || !bind(mesh, x, fy->comps, "gbFieldAxpy") || !flush_for(x) ||
+        !flush_for(y))
+        return 1;
+    launch_field_axpy(impl(mesh)->dev, fy->comps, a, fx->val[fx->cur], fy->val[fy->cur], t_stream);
+    return launch_ok("gbFieldAxpy") ? 0 : 1;
 }
 
 int gbFvmGradient(cuMesh* mesh, FvmField* u) {

@@ -152,6 +152,19 @@ __global__ void k_field_bc(uint32_t g0, uint32_t g1, uint32_t N, const uint2* __
     }
 }
 
+// y += a x over the interior cells (scalar: s, vector: v arrays)
+__global__ void k_field_axpy(uint32_t N, float a, const float* __restrict__ xs, float* ys, const float4* __restrict__ xv,
+                             float4* yv) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    if (ys) {
+        ys[i] = ys[i] + a * xs[i];
+    } else {
+        const float4 x = xv[i], y = yv[i];
+        yv[i] = make_float4(y.x + a * x.x, y.y + a * x.y, y.z + a * x.z, y.w);
+    }
+}
+
 inline unsigned grid_n(int64_t n) { return (unsigned)((n + kBlock - 1) / kBlock); }
 
 }  // namespace
@@ -208,6 +221,15 @@ void launch_field_bc(const DevMesh& m, uint32_t g0, uint32_t g1, int comps, int 
     else
         k_field_bc<<<grid_n(g1 - g0), kBlock, 0, st>>>(g0, g1, (uint32_t)m.N, m.ghost, zero_grad, cur, nullptr, nullptr,
                                                        (float4*)val0, (float4*)val1, value);
+    count_launch();
+}
+
+void launch_field_axpy(const DevMesh& m, int comps, float a, const void* x, void* y, cudaStream_t st) {
+    if (m.N == 0) return;
+    if (comps == 1)
+        k_field_axpy<<<grid_n(m.N), kBlock, 0, st>>>((uint32_t)m.N, a, (const float*)x, (float*)y, nullptr, nullptr);
+    else
+        k_field_axpy<<<grid_n(m.N), kBlock, 0, st>>>((uint32_t)m.N, a, nullptr, nullptr, (const float4*)x, (float4*)y);
     count_launch();
 }
 

@@ -486,6 +486,9 @@ int gbFvmApply(cuMesh* mesh, int op, FvmField* u, FvmField* phi, gb_vector phi_c
 int gbFieldInit(cuMesh* mesh, FvmField* u, gb_vector value);
 int gbFieldBcFixed(cuMesh* mesh, FvmField* u, gb_vector value, unsigned int region_id);
 int gbFieldBcZeroGrad(cuMesh* mesh, FvmField* u, unsigned int region_id);
+/* y += a x over the interior cells (an explicit update with a residual from
+ * gbFvmApplyTerms); x and y of the same kind, distinct. */
+int gbFieldAxpy(cuMesh* mesh, FvmField* y, gb_scalar a, FvmField* x);
 
 /* gbFvmApplyTerms: sum over terms of coef x operator at every interior cell,
  * the operators composed in one pass over each cell's faces (as a model
