@@ -352,6 +352,17 @@ def run_ours(args, rank, world, local_rank):
         ttr = {"reached": reached, "iterations": it, "seconds": c0.elapsed_time(c1) * 1e-3 * it / len(h),
                "min_residual_ratio": float(np.min(ratio)), "max_iterations": args.max_iters,
                "metric": "sum over cells of (F_rho^2+|F_rhou|^2+F_rhoE^2) V, relative to iteration 0"}
+        # the density residual's L2 norm, sqrt(sum of F_rho^2 V), over the
+        # same iterates (gbEulerRunDensityResidual), for args.max_iters
+        case.init(mach, P_INF, T_INF)
+        _, dens = case.run_density(bcs, CFL, args.max_iters, check_every=1000)
+        dl2 = np.sqrt(dens / dens[0])
+        hit = bool(np.any(dl2 < 1e-3))
+        ttr["density_l2"] = {
+            "ratio_at_the_stop": float(dl2[it - 1]) if it <= len(dl2) else None,
+            "min_ratio": float(np.min(dl2)), "iterations_run": int(len(dl2)),
+            "iterations_to_1e-3": int(np.argmax(dl2 < 1e-3)) + 1 if hit else None,
+            "metric": "sqrt(sum over cells of F_rho^2 V), relative to iteration 0"}
 
     # ---- batched sweep (config 3) and learned warm start (config 4), one GPU ----
     batch = warm = None

@@ -105,6 +105,9 @@ _PROTOS = {
     "gbMeshFromSu2": (MeshP, [C.c_char_p]),
     "gbEulerRun": (C.c_int64, [MeshP, FieldP, FieldP, FieldP, FieldP, C.c_float, C.c_int64, C.POINTER(gbBc), C.c_int,
                                C.c_double, C.c_int, C.POINTER(C.c_double)]),
+    "gbEulerRunDensityResidual": (C.c_int64, [MeshP, FieldP, FieldP, FieldP, FieldP, C.c_float, C.c_int64,
+                                              C.POINTER(gbBc), C.c_int, C.c_double, C.c_int,
+                                              C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     "gbKernelLaunchCount": (C.c_uint64, []),
     "gbReduceSumNoAlloc": (C.c_int, [C.c_void_p, C.c_uint64, C.c_void_p, C.c_void_p]),
     "gbBatchCreate": (C.c_void_p, [C.c_int, C.POINTER(MeshP), C.c_int, C.POINTER(gbBatchInstance)]),

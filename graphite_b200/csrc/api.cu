@@ -74,6 +74,7 @@ struct RunGraphs {
     RunCtl* h_ctl = nullptr;          // pinned host copy
     int64_t cap = 0;
     int per_iter = 0;
+    int n_hist = 1;                   // histories of `cap` entries each in `hist`
     void release() {
         for (int k = 0; k < 2; ++k)
             if (exec[k]) cudaGraphExecDestroy(exec[k]);
@@ -479,13 +480,13 @@ FaceRecs recs_of(FvmField* rho, FvmField* rhou) {
 }
 
 void enqueue_flux(cuMesh* mesh, FvmField* rho, FvmField* rhou, FvmField* rhoe, FvmField* error, float cfl, int cur,
-                  cudaStream_t s, const DevMesh* dm = nullptr) {
+                  cudaStream_t s, const DevMesh* dm = nullptr, double* partials_rho = nullptr) {
     MeshImpl* mi = impl(mesh);
     const int nxt = 1 - cur;
     FieldImpl* ei = impl(error);
     launch_flux(dm ? *dm : mi->dev, state_of(rho, rhou, rhoe, cur), recs_of(rho, rhou), (float*)impl(rho)->val[nxt],
                 (float4*)impl(rhou)->val[nxt], (float*)impl(rhoe)->val[nxt], (float*)ei->val[ei->cur], ei->partials,
-                cfl, s);
+                cfl, s, partials_rho);
 }
 
 // Reference-order host copy of the current values.
@@ -575,17 +576,18 @@ void key_bytes(std::vector<uint64_t>& k, const void* p, size_t n) {
 // capacity changed.
 template <class Enqueue>
 bool ensure_run_graphs(MeshImpl* mi, RunGraphs& rg, std::vector<uint64_t>& key, int64_t need, int per_iter,
-                       Enqueue&& enqueue, const char* what) {
-    if (rg.exec[0] && rg.exec[1] && rg.key == key && rg.cap >= need) return true;
+                       Enqueue&& enqueue, const char* what, int n_hist = 1) {
+    if (rg.exec[0] && rg.exec[1] && rg.key == key && rg.cap >= need && rg.n_hist == n_hist) return true;
     const int64_t cap = std::max<int64_t>(need, std::max<int64_t>(256, rg.cap));
     rg.release();
     if (!mi->capture && !cuda_ok(cudaStreamCreateWithFlags(&mi->capture, cudaStreamNonBlocking), what)) return false;
-    if (!dalloc(rg.hist, (size_t)cap, what) || !dalloc(rg.ctl, 1, what) ||
+    if (!dalloc(rg.hist, (size_t)(cap * n_hist), what) || !dalloc(rg.ctl, 1, what) ||
         !cuda_ok(cudaMallocHost((void**)&rg.h_ctl, sizeof(RunCtl)), what)) {
         rg.release();
         return false;
     }
     rg.cap = cap;
+    rg.n_hist = n_hist;
     DevMesh dh = mi->dev;          // the iteration kernels of this loop stop on the halt word
     dh.halt = &rg.ctl->halt;
     bool ok = true;
@@ -614,7 +616,7 @@ bool ensure_run_graphs(MeshImpl* mi, RunGraphs& rg, std::vector<uint64_t>& key, 
 // the tolerance is met), or -1 when a residual was not finite (an error);
 // `cur` becomes the buffer holding the last state.
 int64_t replay_run_graphs(RunGraphs& rg, int& cur, int64_t n_iter, int64_t check_every, std::vector<double>& hist,
-                          cudaStream_t s, const char* what) {
+                          cudaStream_t s, const char* what, std::vector<double>* hist2 = nullptr) {
     const int cur0 = cur;
     int64_t done = 0;
     bool ok = cuda_ok(cudaMemsetAsync(rg.ctl, 0, sizeof(RunCtl), s), what);
@@ -630,6 +632,9 @@ int64_t replay_run_graphs(RunGraphs& rg, int& cur, int64_t n_iter, int64_t check
         if (!ok) break;
         ok = cuda_ok(cudaMemcpyAsync(hist.data() + done, rg.hist, (size_t)chunk * sizeof(double),
                                      cudaMemcpyDeviceToHost, s), what) &&
+             (!hist2 || rg.n_hist < 2 ||
+              cuda_ok(cudaMemcpyAsync(hist2->data() + done, rg.hist + rg.cap, (size_t)chunk * sizeof(double),
+                                      cudaMemcpyDeviceToHost, s), what)) &&
              cuda_ok(cudaMemcpyAsync(rg.h_ctl, rg.ctl, sizeof(RunCtl), cudaMemcpyDeviceToHost, s), what) &&
              cuda_ok(cudaStreamSynchronize(s), what);
         if (!ok) break;
@@ -969,9 +974,9 @@ gb_scalar FvmFieldReduceSum(cuMesh* mesh, FvmField* var) {
     return (gb_scalar)*h;
 }
 
-int64_t gbEulerRun(cuMesh* mesh, FvmField* rho, FvmField* rhou, FvmField* rhoe, FvmField* error, gb_scalar cfl,
-                   int64_t n_iter, const gbBc* bcs, int n_bc, double tolerance, int check_every,
-                   double* residual_history) {
+static int64_t euler_run(cuMesh* mesh, FvmField* rho, FvmField* rhou, FvmField* rhoe, FvmField* error, gb_scalar cfl,
+                         int64_t n_iter, const gbBc* bcs, int n_bc, double tolerance, int check_every,
+                         double* residual_history, double* density_history) {
     clear_error();
     if (n_iter < 0 || n_bc < 0 || (n_bc > 0 && !bcs)) { set_error("gbEulerRun: bad arguments"); return -1; }
     if (!euler_fields(mesh, rho, rhou, rhoe, "gbEulerRun") || !bind(mesh, error, 1, "gbEulerRun") ||
@@ -988,7 +993,8 @@ int64_t gbEulerRun(cuMesh* mesh, FvmField* rho, FvmField* rhou, FvmField* rhoe, 
     if (!ensure_grad(mesh, rho) || !ensure_grad(mesh, rhou) || !ensure_grad(mesh, rhoe)) return -1;
     FieldImpl* ei = impl(error);
     const int nb = (int)((mi->dev.N + kBlock - 1) / kBlock);
-    if (!ensure_partials(ei, std::max(nb, 1))) return -1;
+    const bool density = density_history != nullptr;   // the density residual's partials follow the residual's
+    if (!ensure_partials(ei, std::max(nb, 1) * (density ? 2 : 1))) return -1;
     if (check_every <= 0) check_every = 100;
     cudaStream_t s = t_stream;
     double* out = mi->dev.red + mi->dev.n_red_max;
@@ -1030,6 +1036,7 @@ int64_t gbEulerRun(cuMesh* mesh, FvmField* rho, FvmField* rhou, FvmField* rhoe, 
     key.push_back((uint64_t)n_bc);
     if (n_bc > 0) key_bytes(key, bcs, sizeof(gbBc) * (size_t)n_bc);
     key_bytes(key, &tolerance, sizeof(tolerance));
+    key.push_back((uint64_t)density);
     // one graph per value buffer parity: BCs, gradients+limiters, flux+update, residual
     auto enqueue = [&](int k, cudaStream_t cap, const DevMesh& dh, RunCtl* ctl, double* hist,
                        unsigned long long hcap) {
@@ -1041,16 +1048,18 @@ int64_t gbEulerRun(cuMesh* mesh, FvmField* rho, FvmField* rhou, FvmField* rhoe, 
         }
         launch_grad_lim(dh, state_of(rho, rhou, rhoe, k), grad_of(rho, rhou, rhoe, false), transposed, cap,
                         inline_bcs ? &gbt : nullptr);
-        enqueue_flux(mesh, rho, rhou, rhoe, error, cfl, k, cap, &dh);
+        enqueue_flux(mesh, rho, rhou, rhoe, error, cfl, k, cap, &dh, density ? ei->partials + nb : nullptr);
+        if (density) launch_reduce_history(nb, ei->partials + nb, ctl, hist + hcap, hcap, cap);
         launch_reduce_final(nb, ei->partials, out, cap, ctl, hist, hcap, tolerance);
     };
-    const int per_iter = (inline_bcs ? 0 : (table_bcs ? (n_bc > 0 ? 1 : 0) : n_bc)) + 3;
+    const int per_iter = (inline_bcs ? 0 : (table_bcs ? (n_bc > 0 ? 1 : 0) : n_bc)) + 3 + (density ? 1 : 0);
     if (!ensure_run_graphs(mi, mi->euler_run, key, std::min<int64_t>(check_every, n_iter), per_iter, enqueue,
-                           "gbEulerRun"))
+                           "gbEulerRun", density ? 2 : 1))
         return -1;
     int cur = impl(rho)->cur;
-    std::vector<double> hist((size_t)n_iter, 0.0);
-    const int64_t done = replay_run_graphs(mi->euler_run, cur, n_iter, check_every, hist, s, "gbEulerRun");
+    std::vector<double> hist((size_t)n_iter, 0.0), hist_rho(density ? (size_t)n_iter : 0, 0.0);
+    const int64_t done = replay_run_graphs(mi->euler_run, cur, n_iter, check_every, hist, s, "gbEulerRun",
+                                           density ? &hist_rho : nullptr);
     if (done > 0 && inline_bcs) {
         // the ghost states of the last gradient pass, from the state it read
         // (the buffer before the last update), into both value buffers
@@ -1060,7 +1069,27 @@ int64_t gbEulerRun(cuMesh* mesh, FvmField* rho, FvmField* rhou, FvmField* rhoe, 
     impl(rho)->cur = impl(rhou)->cur = impl(rhoe)->cur = cur;
     ei->partials_valid = true;
     if (residual_history && done > 0) memcpy(residual_history, hist.data(), (size_t)done * sizeof(double));
+    if (density_history && done > 0) memcpy(density_history, hist_rho.data(), (size_t)done * sizeof(double));
     return done;
+}
+
+int64_t gbEulerRun(cuMesh* mesh, FvmField* rho, FvmField* rhou, FvmField* rhoe, FvmField* error, gb_scalar cfl,
+                   int64_t n_iter, const gbBc* bcs, int n_bc, double tolerance, int check_every,
+                   double* residual_history) {
+    return euler_run(mesh, rho, rhou, rhoe, error, cfl, n_iter, bcs, n_bc, tolerance, check_every, residual_history,
+                     nullptr);
+}
+
+int64_t gbEulerRunDensityResidual(cuMesh* mesh, FvmField* rho, FvmField* rhou, FvmField* rhoe, FvmField* error,
+                                  gb_scalar cfl, int64_t n_iter, const gbBc* bcs, int n_bc, double tolerance,
+                                  int check_every, double* residual_history, double* density_history) {
+    if (!density_history) {
+        clear_error();
+        set_error("gbEulerRunDensityResidual: null density history");
+        return -1;
+    }
+    return euler_run(mesh, rho, rhou, rhoe, error, cfl, n_iter, bcs, n_bc, tolerance, check_every, residual_history,
+                     density_history);
 }
 
 }  // extern "C"

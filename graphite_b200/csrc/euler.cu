@@ -179,15 +179,25 @@ void launch_staged(const DevMesh& d, const MeshDev& md, EulerState q, EulerGrad 
 
 // Fused flux / local-time-step update / squared residual over the interior
 // cells of one mesh, with the residual summed per block in float64.
+// RHO: also the density part of each cell's residual, F_rho^2 V, summed per
+// block into partials_rho.
+template <bool RHO>
 __global__ void __launch_bounds__(kBlock, kFluxBlocksPerSM)
     k_flux(MeshDev m, EulerState q, FaceRecs r, float* __restrict__ rho_n, float4* __restrict__ rhou_n,
-           float* __restrict__ rhoe_n, float* __restrict__ err, double* __restrict__ partials, float cfl) {
+           float* __restrict__ rhoe_n, float* __restrict__ err, double* __restrict__ partials, float cfl,
+           double* __restrict__ partials_rho) {
     if (halted(m.halt)) return;              // uniform over the grid
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     double res = 0.0;
-    if (i < m.N) res = (double)flux_cell(m, q, r, rho_n, rhou_n, rhoe_n, err, cfl, i);
+    float rsq = 0.f;
+    if (i < m.N) res = (double)flux_cell(m, q, r, rho_n, rhou_n, rhoe_n, err, cfl, i, RHO ? &rsq : nullptr);
     const double bs = block_sum(res);
     if (threadIdx.x == 0) partials[blockIdx.x] = bs;
+    if (RHO) {
+        __syncthreads();                     // block_sum's scratch is reused
+        const double br = block_sum((double)rsq);
+        if (threadIdx.x == 0) partials_rho[blockIdx.x] = br;
+    }
 }
 
 // one-off setup of the static per-entry geometry
@@ -202,6 +212,20 @@ __global__ void k_reduce_partials(int64_t n, const float* __restrict__ v, double
         s += (double)v[i];
     const double bs = block_sum(s);
     if (threadIdx.x == 0) partials[blockIdx.x] = bs;
+}
+
+// The sum of the partials into history[ctl->it_chunk] (the iteration the
+// next k_reduce_final records), k_reduce_final's order; nothing once halted.
+__global__ void k_reduce_history(int n, const double* __restrict__ partials, const RunCtl* ctl, double* history,
+                                 unsigned long long history_cap) {
+    if (*(const volatile int*)&ctl->halt) return;   // uniform over the block
+    double s = 0.0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) s += partials[i];
+    const double bs = block_sum(s);
+    if (threadIdx.x == 0) {
+        const unsigned long long it = ctl->it_chunk;
+        if (it < history_cap) history[it] = bs;
+    }
 }
 
 __global__ void k_reduce_final(int n, const double* __restrict__ partials, double* out, RunCtl* ctl, double* history,
@@ -315,9 +339,20 @@ void launch_grad_lim(const DevMesh& m, EulerState q, EulerGrad g, bool transpose
 }
 
 void launch_flux(const DevMesh& m, EulerState q, FaceRecs r, float* rho_n, float4* rhou_n, float* rhoe_n,
-                 float* err, double* partials, float cfl, cudaStream_t s) {
+                 float* err, double* partials, float cfl, cudaStream_t s, double* partials_rho) {
     if (m.N == 0) return;
-    k_flux<<<grid(m.N), kBlock, 0, s>>>(mesh_dev(m), q, r, rho_n, rhou_n, rhoe_n, err, partials, cfl);
+    if (partials_rho)
+        k_flux<true><<<grid(m.N), kBlock, 0, s>>>(mesh_dev(m), q, r, rho_n, rhou_n, rhoe_n, err, partials, cfl,
+                                                  partials_rho);
+    else
+        k_flux<false><<<grid(m.N), kBlock, 0, s>>>(mesh_dev(m), q, r, rho_n, rhou_n, rhoe_n, err, partials, cfl,
+                                                   nullptr);
+    count_launch();
+}
+
+void launch_reduce_history(int n_partials, const double* partials, const RunCtl* ctl, double* history,
+                           unsigned long long history_cap, cudaStream_t s) {
+    k_reduce_history<<<1, kBlock, 0, s>>>(n_partials, partials, ctl, history, history_cap);
     count_launch();
 }
 

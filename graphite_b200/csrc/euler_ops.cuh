@@ -406,11 +406,11 @@ __device__ __forceinline__ void grad_lim_cell(const MeshDev& m, EulerState q, Eu
 // with eig = max(|u| + c) over both sides, accumulate eig A / V; then
 // dt = cfl / sum, q_new = q - F dt (into the other buffer).  Returns the
 // squared residual (F_rho^2 + |F_rhou|^2 + F_rhoE^2) V, also stored in err[i]
-// when err is not null.
+// when err is not null; with rho_sq, also the density part F_rho^2 V.
 template <typename Ld = LdNc>
 __device__ __forceinline__ float flux_cell(const MeshDev& m, EulerState q, FaceRecs rec, float* __restrict__ rho_n,
                                            float4* __restrict__ rhou_n, float* __restrict__ rhoe_n,
-                                           float* __restrict__ err, float cfl, uint32_t i) {
+                                           float* __restrict__ err, float cfl, uint32_t i, float* rho_sq = nullptr) {
     const float vol = __ldg(&m.cell_geo[i]).w;
     float fr = 0.f, fe = 0.f, dts = 0.f;
     float3 fu = make_float3(0.f, 0.f, 0.f);
@@ -451,6 +451,9 @@ __device__ __forceinline__ float flux_cell(const MeshDev& m, EulerState q, FaceR
     rhoe_n[i] = e0 - fe * dt;
     const float e = (fr * fr + dot(fu, fu) + fe * fe) * vol;
     if (err) err[i] = e;
+    // explicitly rounded, so that the residual e above compiles as it does
+    // without this output
+    if (rho_sq) *rho_sq = __fmul_rn(__fmul_rn(fr, fr), vol);
     return e;
 }
 

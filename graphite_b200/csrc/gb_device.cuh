@@ -162,8 +162,14 @@ struct NsiGhostTable {
     float* p[2];
     float4* u[2];
 };
+// partials_rho (may be null): also the per-block sums of the density part
+// F_rho^2 V of the residual
 void launch_flux(const DevMesh& m, EulerState q, FaceRecs r, float* rho_n, float4* rhou_n, float* rhoe_n,
-                 float* err, double* partials, float cfl, cudaStream_t s);
+                 float* err, double* partials, float cfl, cudaStream_t s, double* partials_rho = nullptr);
+// the sum of the partials into history[ctl->it_chunk], before the iteration's
+// k_reduce_final (which advances it_chunk)
+void launch_reduce_history(int n_partials, const double* partials, const RunCtl* ctl, double* history,
+                           unsigned long long history_cap, cudaStream_t s);
 void launch_reduce_partials(int64_t n, const float* v, double* partials, cudaStream_t s);
 // stage 1 with a caller-chosen number of blocks (one partial per block)
 void launch_reduce_partials_blocks(int64_t n, const float* v, double* partials, int blocks, cudaStream_t s);

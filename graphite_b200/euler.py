@@ -150,6 +150,20 @@ class EulerCase:
             raise capi.GraphiteError(f"gbEulerRun failed: {capi.last_error()}")
         return hist[:done]
 
+    def run_density(self, bcs, cfl: float, n_iter: int, tolerance: float = 0.0, check_every: int = 100):
+        """run() that also returns the density part of the residual per
+        iteration (sum of F_rho^2 V): (residual history, density history)."""
+        arr = self.bc_structs(bcs)
+        hist = np.zeros(max(n_iter, 1), dtype=np.float64)
+        dens = np.zeros(max(n_iter, 1), dtype=np.float64)
+        done = self.lib.gbEulerRunDensityResidual(self.mesh, self.rho, self.rhou, self.rhoe, self.error, cfl, n_iter,
+                                                  arr, len(bcs), tolerance, check_every,
+                                                  hist.ctypes.data_as(C.POINTER(C.c_double)),
+                                                  dens.ctypes.data_as(C.POINTER(C.c_double)))
+        if done < 0:
+            raise capi.GraphiteError(f"gbEulerRunDensityResidual failed: {capi.last_error()}")
+        return hist[:done], dens[:done]
+
     def fields(self) -> Tuple[np.ndarray, np.ndarray, np.ndarray]:
         """(rho, rhou, rhoe) in reference order, cells then ghosts."""
         out = []

@@ -291,6 +291,15 @@ int64_t gbEulerRun(cuMesh* mesh, FvmField* rho, FvmField* rhou, FvmField* rhoe, 
                    gb_scalar cfl, int64_t n_iter, const gbBc* bcs, int n_bc, double tolerance,
                    int check_every, double* residual_history);
 
+/* gbEulerRun that also writes, per iteration, the density part of the
+ * residual, sum over cells of F_rho^2 V (float64, fixed order), to
+ * density_history (host array of n_iter doubles; its square root relative
+ * to the first is the density residual's L2 drop).  The iterates, the
+ * residual history and the stop test are gbEulerRun's. */
+int64_t gbEulerRunDensityResidual(cuMesh* mesh, FvmField* rho, FvmField* rhou, FvmField* rhoe, FvmField* error,
+                                  gb_scalar cfl, int64_t n_iter, const gbBc* bcs, int n_bc, double tolerance,
+                                  int check_every, double* residual_history, double* density_history);
+
 /* Launches of this library's kernels since load (for accounting). */
 uint64_t gbKernelLaunchCount(void);
 

@@ -360,7 +360,7 @@ struct Solver : SolverBase {
     std::vector<V3<T>> cc, fc, fn;
     std::vector<T> cv, fa;
     std::vector<T3<T>> mat;
-    std::vector<T> rho, rhoe, rho_n, rhoe_n, err;
+    std::vector<T> rho, rhoe, rho_n, rhoe_n, err, err_rho;   // err_rho: the density part F_rho^2 V
     std::vector<V3<T>> rhou, rhou_n;
     std::vector<V3<T>> g_rho, g_rhoe;   // gradients
     std::vector<T3<T>> g_rhou;
@@ -389,6 +389,7 @@ struct Solver : SolverBase {
         rho.assign(NG, 0); rhoe.assign(NG, 0); rhou.assign(NG, mk<T>(0, 0, 0));
         rho_n = rho; rhoe_n = rhoe; rhou_n = rhou;
         err.assign(NG, 0);
+        err_rho.assign(NG, 0);
         g_rho.assign(NG, mk<T>(0, 0, 0)); g_rhoe = g_rho;
         g_rhou.assign(NG, T3<T>{mk<T>(0, 0, 0), mk<T>(0, 0, 0), mk<T>(0, 0, 0)});
         l_rho.assign(NG, 1); l_rhoe.assign(NG, 1); l_rhou.assign(NG, mk<T>(1, 1, 1));
@@ -592,6 +593,7 @@ struct Solver : SolverBase {
             rhou_n[c0] = rhou[c0] - fu * dt;
             rhoe_n[c0] = rhoe[c0] - fe * dt;
             err[c0] = (fr * fr + dot(fu, fu) + fe * fe) * v;
+            err_rho[c0] = fr * fr * v;
         }
         for (int64_t c = b0; c < b1; ++c) { rho[c] = rho_n[c]; rhou[c] = rhou_n[c]; rhoe[c] = rhoe_n[c]; }
     }
@@ -727,7 +729,7 @@ void orc_set_state(void* hp, const double* rho, const double* rhou, const double
 }
 
 // Named solver arrays in reference layout, as float64 (n = N + G entries):
-// rho, rhoe, err, lim_rho, lim_rhoe (1 per cell); rhou, lim_rhou, grad_rho,
+// rho, rhoe, err, err_rho, lim_rho, lim_rhoe (1 per cell); rhou, lim_rhou, grad_rho,
 // grad_rhoe (3); grad_rhou (9: columns u, v, w = gradients of each component).
 int64_t orc_get(void* hp, const char* name, double* out) {
     Handle* h = static_cast<Handle*>(hp);
@@ -742,6 +744,7 @@ int64_t orc_get(void* hp, const char* name, double* out) {
         if (n == "rho") return s1(s->rho);
         if (n == "rhoe") return s1(s->rhoe);
         if (n == "err") return s1(s->err);
+        if (n == "err_rho") return s1(s->err_rho);
         if (n == "lim_rho") return s1(s->l_rho);
         if (n == "lim_rhoe") return s1(s->l_rhoe);
         if (n == "rhou") return s3(s->rhou);

@@ -154,7 +154,7 @@ class OracleSolver:
         assert r.size == self.n and u.size == 3 * self.n and e.size == self.n
         load().orc_set_state(self.h, _ptr(r), _ptr(u), _ptr(e))
 
-    _COMPS = {"rho": 1, "rhoe": 1, "err": 1, "lim_rho": 1, "lim_rhoe": 1, "rhou": 3, "lim_rhou": 3,
+    _COMPS = {"rho": 1, "rhoe": 1, "err": 1, "err_rho": 1, "lim_rho": 1, "lim_rhoe": 1, "rhou": 3, "lim_rhou": 3,
               "grad_rho": 3, "grad_rhoe": 3, "grad_rhou": 9}
 
     def get(self, name: str) -> np.ndarray:

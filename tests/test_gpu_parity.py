@@ -336,3 +336,29 @@ def test_deferred_boundary_conditions(su2_paths):
         assert np.array_equal(np.float32(hg), np.float32(hp))
         for a, b in zip(per_call, graph):
             assert np.array_equal(a, b)
+
+
+def test_density_residual_history(su2_paths):
+    """gbEulerRunDensityResidual: the same iterates and residual history as
+    gbEulerRun (bitwise), and per iteration the density part of the residual,
+    sum of F_rho^2 V, against the float64 oracle's."""
+    iters = 60
+    with EulerCase(su2_paths("tet_12x6x2")) as a, EulerCase(su2_paths("tet_12x6x2")) as b:
+        for c in (a, b):
+            c.init(*INIT)
+        h = a.run(BCS, 0.8, iters)
+        h2, d = b.run_density(BCS, 0.8, iters)
+        assert np.array_equal(h, h2)
+        for x, y in zip(a.fields(), b.fields()):
+            assert np.array_equal(x, y)
+        assert np.all(d > 0) and np.all(d < h)
+    om, s = oracle_state("tet_12x6x2")
+    s.init(*INIT)
+    d64 = []
+    for _ in range(iters):
+        s.apply_bcs(BCS)
+        s.prepare()
+        s.step(0.8)
+        d64.append(float(np.sum(s.get("err_rho")[: om.N])))
+    d64 = np.array(d64)
+    assert np.max(np.abs(d - d64) / d64) < 1e-3, np.max(np.abs(d - d64) / d64)
