@@ -136,6 +136,9 @@ def test_converter_errors(workdir):
     assert "cannot open" in capi.last_error()
     p = _write(str(workdir / "dim2.su2"), "NDIME= 2\n")
     assert lib.cuMeshFromSu2(p.encode(), out) != 0 and "3D" in capi.last_error()
+    # no elements at all
+    p = _write(str(workdir / "empty.su2"), "NDIME= 3\nNELEM= 0\nNPOIN= 0\nNMARK= 0\n")
+    assert lib.cuMeshFromSu2(p.encode(), out) != 0 and "no elements" in capi.last_error()
     # a single tet with no boundary markers: open mesh
     tet = "NDIME= 3\nNELEM= 1\n10 0 1 2 3 0\nNPOIN= 4\n0 0 0 0\n1 0 0 1\n0 1 0 2\n0 0 1 3\n"
     p = _write(str(workdir / "open.su2"), tet)

@@ -362,3 +362,31 @@ def test_density_residual_history(su2_paths):
         d64.append(float(np.sum(s.get("err_rho")[: om.N])))
     d64 = np.array(d64)
     assert np.max(np.abs(d - d64) / d64) < 1e-3, np.max(np.abs(d - d64) / d64)
+
+
+def test_single_cell_mesh(workdir):
+    """The smallest mesh: one tet and its four ghosts (one block of every
+    kernel, most of it idle).  Ten iterations through the per-call loop and
+    the replayed graphs agree bitwise, and with the float64 oracle."""
+    from graphite_b200 import meshgen
+    nodes = np.array([[0, 0, 0], [1, 0, 0], [0, 1, 0], [0, 0, 1]], np.float32)
+    em = meshgen.ElementMesh(nodes, [(meshgen.TET, np.array([[0, 1, 2, 3]]))],
+                             {"wall": [(meshgen.TRI, np.array([[0, 2, 1], [0, 1, 3]]))],
+                              "farfield": [(meshgen.TRI, np.array([[1, 2, 3], [0, 3, 2]]))]}, name="one_tet")
+    path = str(workdir / "one_tet.su2")
+    em.write_su2(path)
+    bcs = [("slip", "wall"), ("farfield", "farfield", 0.5, 0.0, 0.1, cases.P_INF, cases.T_INF)]
+    with EulerCase(path) as a, EulerCase(path) as b:
+        assert a.n_cells == 1 and a.n_ghosts == 4
+        for c in (a, b):
+            c.init((0.4, 0.0, 0.05), cases.P_INF, cases.T_INF)
+        h = np.array([a.iterate(bcs, 0.5) for _ in range(10)])
+        h2 = b.run(bcs, 0.5, 10)
+        np.testing.assert_array_equal(h, h2)
+        for x, y in zip(a.fields(), b.fields()):
+            np.testing.assert_array_equal(x, y)
+        s = OracleSolver(OracleMesh(em, metric_bits=64), bits=64)
+        s.init((0.4, 0.0, 0.05), cases.P_INF, cases.T_INF)
+        h64 = s.run(bcs, 10, 0.5)
+        np.testing.assert_allclose(h, h64, rtol=1e-4)
+        assert rel_max(a.fields()[0][:1], s.get("rho")[:1]) < 1e-5
