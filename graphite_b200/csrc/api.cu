@@ -175,6 +175,13 @@ void free_mesh(cuMesh* m) {
 // Topology -> device mesh + host mirror.
 cuMesh* create_mesh(Topology&& topo) {
     cudaStream_t s = t_stream;
+    // every device index is 32-bit: cells with ghosts, faces, and the
+    // per-face entries with the ghosts' face-state slots after them (S + G)
+    if ((uint64_t)kSlots * (uint64_t)topo.N + (uint64_t)topo.G >= (1ull << 32) || (uint64_t)topo.F >= (1ull << 32)) {
+        set_error("mesh too large for 32-bit device indices: " + std::to_string(topo.N) + " cells, " +
+                  std::to_string(topo.G) + " ghosts, " + std::to_string(topo.F) + " faces");
+        return nullptr;
+    }
     cuMesh* m = hmalloc<cuMesh>(1);
     MeshImpl* mi = new MeshImpl();
     m->impl = mi;
