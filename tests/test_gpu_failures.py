@@ -135,3 +135,26 @@ def test_persistent_barrier_that_cannot_complete_is_reported(airfoil):
     for q in range(3):
         assert np.array_equal(got[q], ref[q])
     c.close()
+
+
+def test_nsi_non_finite_state_is_reported_by_the_run(workdir):
+    """gbNSIRun reports a non-finite residual as an error, like gbEulerRun,
+    and runs normally again from a valid state."""
+    from graphite_b200.nsi import NSICase
+    path = str(workdir / "nsi_fail_cyl.su2")
+    meshgen.cylinder_ogrid(32, 16, ratio=1.15, r_far=10.0).write_su2(path)
+    bcs = [("wall", "cylinder"), ("inletoutlet", "farfield", 1.0, 0.0, 0.0, 0.0), ("slip", "sides")]
+    c = NSICase(path)
+    try:
+        c.init((1.0, 0.0, 0.0), 0.0)
+        u, p = c.fields()
+        bad = p.copy()
+        bad[5] = np.nan
+        c.set_state(u, bad)
+        with pytest.raises(capi.GraphiteError, match="not finite"):
+            c.run(bcs, 0.5, 40, check_every=10)
+        c.set_state(u, p)
+        h = c.run(bcs, 0.5, 40, check_every=10)
+        assert len(h) == 40 and np.all(np.isfinite(h))
+    finally:
+        c.close()
