@@ -569,9 +569,9 @@ int gbNSIWallForce(cuMesh* mesh, FvmField* velocity, FvmField* pressure, unsigne
  * loads the library until exit), so n is limited to 4096 * 2048 = 8,388,608;
  * larger n is rejected with an error.  values and result must be device (or
  * managed) memory; other pointers are rejected.  The first call on each
- * device looks the array up (cudaGetSymbolAddress) and should come before
- * any stream capture; the address it keeps does not survive a
- * cudaDeviceReset of that device.  All calls share the array: calls that
+ * device looks the array's address up (cudaGetSymbolAddress) and keeps it;
+ * that address does not survive a cudaDeviceReset of that device.  All
+ * calls share the array: calls that
  * overlap on the GPU (other streams, other threads) race and must be ordered
  * by the caller.  Asynchronous on `stream` (a cudaStream_t; NULL = legacy
  * default stream).  Returns 0, or nonzero with gbGetLastError set.  No
