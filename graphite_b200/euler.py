@@ -98,13 +98,23 @@ class EulerCase:
         return n * (4 + 12 + 4)
 
     def apply_bcs(self, bcs) -> None:
-        for b in bcs:
-            if b[0] == "slip":
-                rc = self.lib.FvmEulerSlipBc(self.mesh, self.rho, self.rhou, self.rhoe, b[1].encode())
-            else:
-                rc = self.lib.FvmEulerInletOutletBc(self.mesh, self.rho, self.rhou, self.rhoe, capi.vec(b[2:5]),
-                                                    float(b[5]), float(b[6]), b[1].encode())
-            capi.check(rc, f"boundary condition {b[0]} on {b[1]}")
+        # the calls' arguments are built once per list of conditions
+        key = tuple(tuple(b) for b in bcs)
+        if getattr(self, "_bc_key", None) != key:
+            calls = []
+            for b in bcs:
+                if b[0] == "slip":
+                    calls.append((self.lib.FvmEulerSlipBc, (self.mesh, self.rho, self.rhou, self.rhoe,
+                                                            b[1].encode()), b))
+                else:
+                    calls.append((self.lib.FvmEulerInletOutletBc,
+                                  (self.mesh, self.rho, self.rhou, self.rhoe, capi.vec(b[2:5]), float(b[5]),
+                                   float(b[6]), b[1].encode()), b))
+            self._bc_key, self._bc_calls = key, calls
+        for fn, args, b in self._bc_calls:
+            rc = fn(*args)
+            if rc != 0:
+                capi.check(rc, f"boundary condition {b[0]} on {b[1]}")
 
     def prepare(self) -> None:
         capi.check(self.lib.FvmEulerStepPrepare(self.mesh, self.rho, self.rhou, self.rhoe), "FvmEulerStepPrepare")
